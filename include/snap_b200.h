@@ -1,0 +1,146 @@
+/*
+ * snap_b200: B200-native (sm_100a) steady-state solve path of Legion-SNAP.
+ *
+ * A thin C ABI over hand-written CUDA kernels.  Each entry point replaces one
+ * of the reference's task-level operations on the solve path; the reference
+ * implements them as Legion task variants whose GPU bodies call the host
+ * launchers cited beside each declaration (file:line in the reference tree).
+ *
+ * Conventions
+ *  - Every array argument is a DEVICE pointer owned by the caller, except
+ *    where a parameter is documented as host memory.  `stream` is a
+ *    cudaStream_t passed as void*; all work is stream-ordered.
+ *  - Cells are single-chunk, x fastest: c = (z*ny + y)*nx + x.
+ *  - mat[c]: int32, 1-based material id (the reference's mat field).
+ *  - sig[g*nmat + m-1]: per-group, per-material cross section.
+ *  - slgg[((g_to*nmat + m-1)*ng + g_from)*nmom + l]: scattering matrix
+ *    (the reference's slgg field g_to at point (m, g_from), Legendre order l).
+ *  - Per-cell per-group arrays are group-major: xs[g*C + c].
+ *  - Moment arrays hold cmom = nmom*nmom flux moments per cell and group,
+ *    moment 0 being the scalar flux: flux[(g*C + c)*cmom + k].
+ *  - s_xs[(g*C + c)*nmom + l]: in-group scattering per Legendre order.
+ *  - Floating point: SNAP_FP64 arrays are double; SNAP_FP32 contexts take
+ *    float arrays for the sweep-side data (qtot, t_xs, flux) and double for
+ *    the convergence/residual data (see the per-function notes).
+ *  - Every function returns a snap_status; none exits the process.
+ */
+#ifndef SNAP_B200_H
+#define SNAP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  SNAP_OK = 0,
+  SNAP_ERR_BAD_ARG = 1,
+  SNAP_ERR_UNSUPPORTED = 2,
+  SNAP_ERR_OOM = 3,
+  SNAP_ERR_DEVICE_TIMEOUT = 4, /* a bounded device-side wait gave up */
+  SNAP_ERR_CUDA = 5
+} snap_status;
+
+typedef enum { SNAP_FP64 = 0, SNAP_FP32 = 1 } snap_precision;
+
+typedef struct {
+  int nx, ny, nz;      /* cells of the single spatial chunk */
+  int nang;            /* angles per octant */
+  int ng;              /* energy groups */
+  int nmom;            /* Legendre orders (1..4); cmom = nmom*nmom moments */
+  int nmat;            /* materials in the sig/slgg tables */
+  int fixup;           /* negative-flux fixup (sweep.cc:425-518) */
+  int precision;       /* snap_precision */
+  double hi, hj, hk;   /* 2/dx, 2/dy, 2/dz (snap.cc:1178-1180) */
+  /* HOST arrays, copied at create time: quadrature and moment coefficients
+   * (snap.cc:1208-1337; ec laid out [octant][cmom][nang]) */
+  const double *mu, *eta, *xi, *w;
+  const double *ec;
+} snap_config;
+
+typedef struct snap_ctx snap_ctx;
+
+/* Creates a context on `device`: uploads the quadrature, builds the per-octant
+ * coefficient tables and allocates the sweep's scratch (per-octant flux
+ * slots, tile-boundary faces, progress flags).
+ * Replaces InitGPUSweep -> initialize_gpu_context (init.cc:215-236,
+ * gpu_sweep.cu:71-273). */
+int snap_create(const snap_config *cfg, int device, snap_ctx **out);
+int snap_destroy(snap_ctx *ctx);
+
+/* Bytes of device scratch the context holds. */
+size_t snap_scratch_bytes(const snap_ctx *ctx);
+
+/* xs[g*C + c] = sig[g*nmat + mat[c]-1]
+ * Replaces ExpandCrossSection (expxs.cc:118-160 -> run_expand_cross_section,
+ * gpu_expxs.cu:21-267).  Always double. */
+int snap_expand_xs(snap_ctx *ctx, const double *sig, const int32_t *mat, double *xs,
+                   void *stream);
+
+/* s_xs[(g*C + c)*nmom + l] = slgg[g][mat[c]][g][l]
+ * Replaces ExpandScatteringCrossSection (expxs.cc:253-290 ->
+ * run_expand_scattering_cross_section, gpu_expxs.cu:269-534).  Always double. */
+int snap_expand_scattering_xs(snap_ctx *ctx, const double *slgg, const int32_t *mat,
+                              double *s_xs, void *stream);
+
+/* q2grp[(g*C+c)*cmom + 0] = qi[g*C+c] + sum_{g'!=g} slgg[g][mat][g'][0] flux[g'][c][0]
+ * q2grp[(g*C+c)*cmom + k] = sum_{g'!=g} slgg[g][mat][g'][l(k)] flux[g'][c][k]
+ * Replaces CalcOuterSource (outer.cc:220-284 -> run_flux0_outer_source /
+ * run_fluxm_outer_source, gpu_outer.cu:76-441).  Always double. */
+int snap_calc_outer_source(snap_ctx *ctx, const double *qi, const double *slgg,
+                           const int32_t *mat, const double *flux, double *q2grp,
+                           void *stream);
+
+/* qtot[k] = q2grp[k] + flux[k] * s_xs[l(k)]
+ * Replaces CalcInnerSource (inner.cc:163-215 -> run_inner_source_*,
+ * gpu_inner.cu:22-117).  FP64 context: qtot double.  FP32 context: qtot float. */
+int snap_calc_inner_source(snap_ctx *ctx, const double *s_xs, const double *q2grp,
+                           const double *flux, void *qtot, void *stream);
+
+/* One full sweep of all 8 octants and all groups with vacuum boundaries:
+ * flux = sum over octants and angles (zeroed first).  One persistent kernel
+ * covers every octant and group.
+ * Replaces perform_sweeps' MiniKBATask launches (snap.cc:849-887,
+ * sweep.cc:1524-1620 -> run_gpu_sweep, gpu_sweep.cu:2047-2295).
+ * FP64 context: qtot/t_xs/flux double.  FP32 context: float. */
+int snap_sweep(snap_ctx *ctx, const void *qtot, const void *t_xs, void *flux, void *stream);
+
+/* converged = every scalar flux satisfies |flux/prev - 1| <= epsi (or
+ * |flux| <= epsi where |prev| < 1e-12).  kind 0: inner test (epsi as given);
+ * kind 1: outer test, which the caller runs with 100*epsi and only when the
+ * inner loop converged.  `flux`/`prev` hold cmom moments per cell (moment 0
+ * tested).  *converged is HOST memory; the call synchronises `stream`.
+ * Replaces TestInnerConvergence / TestOuterConvergence (inner.cc:327-367,
+ * outer.cc:405-451 -> run_inner_convergence / run_outer_convergence,
+ * gpu_inner.cu:119-236, gpu_outer.cu:443-563).  Always double. */
+int snap_test_convergence(snap_ctx *ctx, int kind, const double *flux, const double *prev,
+                          double epsi, int *converged, void *stream);
+
+typedef struct {
+  double epsi;
+  int iitm, oitm;
+  /* outputs */
+  int inner_total, outer_total, converged;
+  int inners_per_outer[1024];
+  double sweep_ms;     /* device time spent in the sweep kernels */
+  double total_ms;     /* device time of the whole solve */
+} snap_solve_info;
+
+/* Full steady-state fixed-source solve, the sequential semantics of the
+ * reference's predicated loop (snap.cc:409-541): cross-section expansion,
+ * outer source, inner source, sweep, inner/outer convergence.  flux (cmom
+ * moments, double) holds the result; it is zeroed first (snap.cc:313-316).
+ * Replaces Snap::transport_solve's loop body for one time step. */
+int snap_transport_solve(snap_ctx *ctx, const int32_t *mat, const double *qi,
+                         const double *sigt, const double *slgg, const double *sigt_scale,
+                         double *flux, snap_solve_info *info, void *stream);
+
+/* Last error message of this thread (static storage). */
+const char *snap_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,87 @@
+// Internal declarations shared by the CUDA translation units of snap_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "snap_b200.h"
+
+namespace snapb200 {
+
+// Parameters of one launch of the persistent sweep kernel.
+struct SweepParams {
+  int nx, ny, nz;
+  int M;           // flux moments (cmom)
+  int A;           // real angles per octant
+  int G;           // groups
+  int tiles_x, tiles_y;
+  int n_items;     // work items of this launch
+  int o_base;      // first octant of this launch
+  int accumulate;  // add into the flux slots instead of storing
+  int fixup;
+  long long timeout_ns;
+  const int *item_table;  // item -> (sweep << 16) | (tx << 8) | ty
+  const int *item_index;  // [sweep][tx][ty] -> item
+  const void *qtot;       // [G][C][M]
+  const void *t_xs;       // [G][C]
+  void *phi_slots;        // [octants per launch][G][C][M]
+  void *bx;               // [item][nz][TY][AP] x-faces leaving a tile
+  void *by;               // [item][nz][8][AP]  y-faces leaving a tile
+  int *progress;          // [item] completed steps
+  int *counter;           // work-queue head
+  int *error;             // device error word
+  const void *bt1;        // [8][MK][NT][32] source-expansion fragments
+  const void *bt2;        // [8][2NT][MN][32] moment-accumulation fragments
+  const void *coef;       // [4][AP]: hi*mu, hj*eta, hk*xi, w
+};
+
+// Per-precision static configuration picked at context creation.
+struct SweepShape {
+  int NT;   // angle tiles of 8 (AP = 8*NT padded angles)
+  int MK;   // source k-tiles of 4 moments (0: single moment)
+  int MN;   // moment n-tiles of 8
+  int TY;   // warps per CTA = tile rows in y
+};
+
+// Error codes written to the device error word.
+enum : int { DEV_ERR_NONE = 0, DEV_ERR_TIMEOUT = 1 };
+
+// sweep kernels (sweep_fp64.cu / sweep_fp32.cu)
+cudaError_t launch_sweep_fp64(const SweepShape &sh, const SweepParams &p, int grid,
+                              cudaStream_t st);
+cudaError_t sweep_fp64_occupancy(const SweepShape &sh, int *blocks_per_sm, size_t *smem);
+size_t sweep_fp64_smem(const SweepShape &sh);
+bool sweep_fp64_supported(const SweepShape &sh);
+
+cudaError_t launch_sweep_fp32(const SweepShape &sh, const SweepParams &p, int grid,
+                              cudaStream_t st);
+cudaError_t sweep_fp32_occupancy(const SweepShape &sh, int *blocks_per_sm, size_t *smem);
+size_t sweep_fp32_smem(const SweepShape &sh);
+bool sweep_fp32_supported(const SweepShape &sh);
+
+// small kernels (kernels.cu)
+cudaError_t k_expand_xs(const double *sig, const int32_t *mat, double *xs, int G, int nmat,
+                        long long C, cudaStream_t st);
+cudaError_t k_scale_xs(double *xs, const double *scale, int G, long long C, cudaStream_t st);
+cudaError_t k_expand_scat(const double *slgg, const int32_t *mat, double *s_xs, int G, int nmat,
+                          int nmom, long long C, cudaStream_t st);
+cudaError_t k_outer_source(const double *qi, const double *slgg, const int32_t *mat,
+                           const double *flux, double *q2grp, int G, int nmat, int nmom, int M,
+                           long long C, cudaStream_t st);
+cudaError_t k_inner_source(const double *s_xs, const double *q2grp, const double *flux,
+                           void *qtot, int fp32, int G, int nmom, int M, long long C,
+                           cudaStream_t st);
+// flux = sum of `slots` partial slots; optionally counts convergence violations
+// of the new scalar flux against the old one (read before it is overwritten).
+cudaError_t k_reduce_slots(const void *slots, int nslots, int fp32, void *flux_out,
+                           int out_fp32, double *flux64_out, int G, int M, long long C,
+                           int test, double epsi, int *violations, cudaStream_t st);
+cudaError_t k_count_violations(const double *flux, const double *prev, int M, long long n,
+                               double epsi, int *violations, cudaStream_t st);
+cudaError_t k_to_f32(const double *in, float *out, long long n, cudaStream_t st);
+cudaError_t k_copy_moment0(const double *flux, double *out, int M, long long n, cudaStream_t st);
+
+}  // namespace snapb200

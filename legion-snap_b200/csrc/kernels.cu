@@ -1,0 +1,254 @@
+// HBM-bound kernels around the sweep: cross-section expansion, outer and
+// inner sources, the octant-slot reduction fused with the convergence test.
+#include "internal.h"
+
+namespace snapb200 {
+namespace {
+
+constexpr int BLK = 256;
+
+inline int grid_for(long long n, int per_block = BLK) {
+  long long g = (n + per_block - 1) / per_block;
+  if (g > 148LL * 32) g = 148LL * 32;   // grid-stride beyond 32 CTAs per SM
+  return (int)(g < 1 ? 1 : g);
+}
+
+__device__ __forceinline__ int band_of(int k) {
+  int l = 0;
+  while ((l + 1) * (l + 1) <= k) ++l;
+  return l;
+}
+
+// expxs.cc:85-115 / gpu_expxs.cu:21-267
+__global__ void expand_xs_kernel(const double *__restrict__ sig, const int32_t *__restrict__ mat,
+                                 double *__restrict__ xs, int G, int nmat, long long C) {
+  const long long n = (long long)G * C;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int g = (int)(i / C);
+    const long long c = i - (long long)g * C;
+    xs[i] = sig[g * nmat + (mat[c] - 1)];
+  }
+}
+
+__global__ void scale_xs_kernel(double *__restrict__ xs, const double *__restrict__ scale, int G,
+                                long long C) {
+  const long long n = (long long)G * C;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    xs[i] *= scale[i % C];
+}
+
+// expxs.cc:220-250 / gpu_expxs.cu:269-534
+__global__ void expand_scat_kernel(const double *__restrict__ slgg, const int32_t *__restrict__ mat,
+                                   double *__restrict__ s_xs, int G, int nmat, int nmom,
+                                   long long C) {
+  const long long n = (long long)G * C * nmom;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int l = (int)(i % nmom);
+    const long long gc = i / nmom;
+    const int g = (int)(gc / C);
+    const long long c = gc - (long long)g * C;
+    s_xs[i] = slgg[(((size_t)g * nmat + (mat[c] - 1)) * G + g) * nmom + l];
+  }
+}
+
+// outer.cc:107-217 / gpu_outer.cu:22-441, all cmom moments.  A CTA stages
+// the flux of CELLS cells (all groups and moments) in shared memory and
+// produces every (group, cell, moment) output of those cells.
+template <int CELLS>
+__global__ void outer_source_kernel(const double *__restrict__ qi, const double *__restrict__ slgg,
+                                    const int32_t *__restrict__ mat,
+                                    const double *__restrict__ flux, double *__restrict__ q2grp,
+                                    int G, int nmat, int nmom, int M, long long C) {
+  extern __shared__ double sflux[];   // [G][CELLS][M]
+  const long long ntiles = (C + CELLS - 1) / CELLS;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const long long c0 = tile * CELLS;
+    const int nc = (int)min((long long)CELLS, C - c0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < G * CELLS * M; i += blockDim.x) {
+      const int m = i % M, cc = (i / M) % CELLS, g = i / (M * CELLS);
+      sflux[i] = cc < nc ? flux[((size_t)g * C + c0 + cc) * M + m] : 0.0;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < G * CELLS * M; i += blockDim.x) {
+      const int m = i % M, cc = (i / M) % CELLS, g1 = i / (M * CELLS);
+      if (cc >= nc) continue;
+      const long long c = c0 + cc;
+      const int l = band_of(m);
+      const double *row = slgg + ((size_t)g1 * nmat + (mat[c] - 1)) * G * nmom + l;
+      double acc = (m == 0) ? qi[(size_t)g1 * C + c] : 0.0;
+      for (int g2 = 0; g2 < G; ++g2) {
+        if (g2 == g1) continue;
+        acc += __ldg(row + (size_t)g2 * nmom) * sflux[(g2 * CELLS + cc) * M + m];
+      }
+      q2grp[((size_t)g1 * C + c) * M + m] = acc;
+    }
+  }
+}
+
+// inner.cc:106-160 / gpu_inner.cu:22-117
+template <typename QT>
+__global__ void inner_source_kernel(const double *__restrict__ s_xs,
+                                    const double *__restrict__ q2grp,
+                                    const double *__restrict__ flux, QT *__restrict__ qtot, int G,
+                                    int nmom, int M, long long C) {
+  const long long n = (long long)G * C * M;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int m = (int)(i % M);
+    const long long gc = i / M;
+    qtot[i] = (QT)(q2grp[i] + flux[i] * s_xs[gc * nmom + band_of(m)]);
+  }
+}
+
+// flux = sum of the octant slots.  With `test`, also the inner convergence
+// test of inner.cc:283-324 against the previous scalar flux, which is read
+// from flux64_out before it is overwritten.
+template <typename ST, typename OT>
+__global__ void reduce_slots_kernel(const ST *__restrict__ slots, int nslots, OT *flux_out,
+                                    double *flux64_out, int G, int M, long long C, int test,
+                                    double epsi, int *violations) {
+  const long long n = (long long)G * C * M;
+  int bad = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int k = 0; k < nslots; ++k) s += (double)slots[(size_t)k * n + i];
+    if (test && (i % M) == 0) {
+      double prev = flux64_out[i];
+      double df = 1.0;
+      if (fabs(prev) < 1.0e-12) {
+        prev = 1.0;
+        df = 0.0;
+      }
+      df = fabs(s / prev - df);
+      if (df > epsi) ++bad;
+    }
+    if (flux_out) flux_out[i] = (OT)s;
+    if (flux64_out && (void *)flux64_out != (void *)flux_out) flux64_out[i] = s;
+  }
+  if (test) {
+    bad = __reduce_add_sync(0xffffffffu, bad);
+    if ((threadIdx.x & 31) == 0 && bad) atomicAdd(violations, bad);
+  }
+}
+
+// inner.cc:283-324 / outer.cc:354-403
+__global__ void count_violations_kernel(const double *__restrict__ flux,
+                                        const double *__restrict__ prev, int M, long long n,
+                                        double epsi, int *violations) {
+  int bad = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    double p = prev[i * M];
+    double df = 1.0;
+    if (fabs(p) < 1.0e-12) {
+      p = 1.0;
+      df = 0.0;
+    }
+    df = fabs(flux[i * M] / p - df);
+    if (df > epsi) ++bad;
+  }
+  bad = __reduce_add_sync(0xffffffffu, bad);
+  if ((threadIdx.x & 31) == 0 && bad) atomicAdd(violations, bad);
+}
+
+__global__ void copy_moment0_kernel(const double *__restrict__ flux, double *__restrict__ out,
+                                    int M, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i * M] = flux[i * M];
+}
+
+__global__ void to_f32_kernel(const double *__restrict__ in, float *__restrict__ out, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = (float)in[i];
+}
+
+}  // namespace
+
+cudaError_t k_to_f32(const double *in, float *out, long long n, cudaStream_t st) {
+  to_f32_kernel<<<grid_for(n), BLK, 0, st>>>(in, out, n);
+  return cudaGetLastError();
+}
+
+cudaError_t k_expand_xs(const double *sig, const int32_t *mat, double *xs, int G, int nmat,
+                        long long C, cudaStream_t st) {
+  expand_xs_kernel<<<grid_for((long long)G * C), BLK, 0, st>>>(sig, mat, xs, G, nmat, C);
+  return cudaGetLastError();
+}
+
+cudaError_t k_scale_xs(double *xs, const double *scale, int G, long long C, cudaStream_t st) {
+  scale_xs_kernel<<<grid_for((long long)G * C), BLK, 0, st>>>(xs, scale, G, C);
+  return cudaGetLastError();
+}
+
+cudaError_t k_expand_scat(const double *slgg, const int32_t *mat, double *s_xs, int G, int nmat,
+                          int nmom, long long C, cudaStream_t st) {
+  expand_scat_kernel<<<grid_for((long long)G * C * nmom), BLK, 0, st>>>(slgg, mat, s_xs, G, nmat,
+                                                                          nmom, C);
+  return cudaGetLastError();
+}
+
+cudaError_t k_outer_source(const double *qi, const double *slgg, const int32_t *mat,
+                           const double *flux, double *q2grp, int G, int nmat, int nmom, int M,
+                           long long C, cudaStream_t st) {
+  constexpr int CELLS = 4;
+  const size_t smem = sizeof(double) * G * CELLS * M;
+  if (smem > 200 * 1024) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(outer_source_kernel<CELLS>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const long long tiles = (C + CELLS - 1) / CELLS;
+  outer_source_kernel<CELLS><<<grid_for(tiles, 1), BLK, smem, st>>>(qi, slgg, mat, flux, q2grp, G,
+                                                                     nmat, nmom, M, C);
+  return cudaGetLastError();
+}
+
+cudaError_t k_inner_source(const double *s_xs, const double *q2grp, const double *flux, void *qtot,
+                           int fp32, int G, int nmom, int M, long long C, cudaStream_t st) {
+  const int grid = grid_for((long long)G * C * M);
+  if (fp32)
+    inner_source_kernel<float><<<grid, BLK, 0, st>>>(s_xs, q2grp, flux, (float *)qtot, G, nmom, M, C);
+  else
+    inner_source_kernel<double><<<grid, BLK, 0, st>>>(s_xs, q2grp, flux, (double *)qtot, G, nmom, M,
+                                                      C);
+  return cudaGetLastError();
+}
+
+cudaError_t k_reduce_slots(const void *slots, int nslots, int fp32, void *flux_out, int out_fp32,
+                           double *flux64_out, int G, int M, long long C, int test, double epsi,
+                           int *violations, cudaStream_t st) {
+  const int grid = grid_for((long long)G * C * M);
+  if (fp32) {
+    if (out_fp32)
+      reduce_slots_kernel<float, float><<<grid, BLK, 0, st>>>(
+          (const float *)slots, nslots, (float *)flux_out, flux64_out, G, M, C, test, epsi, violations);
+    else
+      reduce_slots_kernel<float, double><<<grid, BLK, 0, st>>>(
+          (const float *)slots, nslots, (double *)flux_out, flux64_out, G, M, C, test, epsi,
+          violations);
+  } else {
+    reduce_slots_kernel<double, double><<<grid, BLK, 0, st>>>(
+        (const double *)slots, nslots, (double *)flux_out, flux64_out, G, M, C, test, epsi,
+        violations);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t k_count_violations(const double *flux, const double *prev, int M, long long n,
+                               double epsi, int *violations, cudaStream_t st) {
+  count_violations_kernel<<<grid_for(n), BLK, 0, st>>>(flux, prev, M, n, epsi, violations);
+  return cudaGetLastError();
+}
+
+cudaError_t k_copy_moment0(const double *flux, double *out, int M, long long n, cudaStream_t st) {
+  copy_moment0_kernel<<<grid_for(n), BLK, 0, st>>>(flux, out, M, n);
+  return cudaGetLastError();
+}
+
+}  // namespace snapb200

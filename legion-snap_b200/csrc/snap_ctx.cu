@@ -1,0 +1,497 @@
+// C ABI of snap_b200: context creation, task-level entry points and the host
+// driver of the steady-state solve loop (a sequential restatement of the
+// reference's predicated loop, snap.cc:409-541).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+#include "snap_b200.h"
+
+using namespace snapb200;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string &msg) {
+  g_last_error = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+  return fail(SNAP_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define SNAP_CUDA(call)                                  \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);  \
+  } while (0)
+
+}  // namespace
+
+struct snap_ctx {
+  snap_config cfg{};
+  std::vector<double> mu, eta, xi, w, ec;
+  int device = 0;
+  int fp32 = 0;
+  int M = 1, A = 1;
+  SweepShape shape{};
+  int AP = 8;
+  int P = 8;            // octants per sweep launch (= flux slots)
+  int tiles_x = 1, tiles_y = 1, n_items = 0;
+  int grid = 0;
+  long long C = 0;
+  long long timeout_ns = 2000000000LL;
+  size_t wsize = 8;     // bytes per sweep-side word
+  // device buffers
+  void *d_coef = nullptr, *d_bt1 = nullptr, *d_bt2 = nullptr;
+  int *d_item_table = nullptr, *d_item_index = nullptr;
+  void *d_slots = nullptr, *d_bx = nullptr, *d_by = nullptr;
+  int *d_ctrl = nullptr;   // [n_items progress][counter][error][violations]
+  int *h_ctrl = nullptr;   // pinned: error, violations
+  size_t scratch_bytes = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  int *progress() { return d_ctrl; }
+  int *counter() { return d_ctrl + n_items; }
+  int *error() { return d_ctrl + n_items + 1; }
+  int *violations() { return d_ctrl + n_items + 2; }
+};
+
+namespace {
+
+void free_ctx(snap_ctx *c) {
+  if (!c) return;
+  cudaFree(c->d_coef);
+  cudaFree(c->d_bt1);
+  cudaFree(c->d_bt2);
+  cudaFree(c->d_item_table);
+  cudaFree(c->d_item_index);
+  cudaFree(c->d_slots);
+  cudaFree(c->d_bx);
+  cudaFree(c->d_by);
+  cudaFree(c->d_ctrl);
+  if (c->h_ctrl) cudaFreeHost(c->h_ctrl);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  delete c;
+}
+
+template <typename T>
+int upload(void **dst, const std::vector<T> &v) {
+  SNAP_CUDA(cudaMalloc(dst, std::max<size_t>(v.size(), 1) * sizeof(T)));
+  SNAP_CUDA(cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return SNAP_OK;
+}
+
+// Per-octant MMA operand tables in the lane order of the m8n8k4 fragments.
+template <typename T>
+void build_tables(const snap_ctx *c, std::vector<T> &coef, std::vector<T> &bt1,
+                  std::vector<T> &bt2) {
+  const int AP = c->AP, NT = c->shape.NT, MK = c->shape.MK, MN = c->shape.MN, M = c->M,
+            A = c->A;
+  coef.assign(4 * AP, T(0));
+  for (int a = 0; a < A; ++a) {
+    coef[a] = (T)(c->cfg.hi * c->mu[a]);
+    coef[AP + a] = (T)(c->cfg.hj * c->eta[a]);
+    coef[2 * AP + a] = (T)(c->cfg.hk * c->xi[a]);
+    coef[3 * AP + a] = (T)c->w[a];
+  }
+  auto ec = [&](int o, int m, int a) { return c->ec[((size_t)o * M + m) * A + a]; };
+  const int B1 = MK * NT * 32, B2 = 2 * NT * MN * 32;
+  bt1.assign((size_t)8 * B1, T(0));
+  bt2.assign((size_t)8 * B2, T(0));
+  for (int o = 0; o < 8; ++o) {
+    for (int kt = 0; kt < MK; ++kt)
+      for (int nt = 0; nt < NT; ++nt)
+        for (int l = 0; l < 32; ++l) {
+          const int m = (l & 3) * MK + kt, a = 8 * nt + (l >> 2);
+          bt1[(size_t)o * B1 + (kt * NT + nt) * 32 + l] = (m < M && a < A) ? (T)ec(o, m, a) : T(0);
+        }
+    for (int t = 0; t < 2 * NT; ++t)
+      for (int mt = 0; mt < MN; ++mt)
+        for (int l = 0; l < 32; ++l) {
+          const int nt = t >> 1, h = t & 1;
+          const int a = 8 * nt + 2 * (l & 3) + h;
+          const int r = l >> 2;
+          const int m = (r >> 1) * 2 * MN + 2 * mt + (r & 1);
+          bt2[(size_t)o * B2 + (t * MN + mt) * 32 + l] =
+              (m < M && a < A) ? (T)(ec(o, m, a) * c->w[a]) : T(0);
+        }
+  }
+}
+
+// Work items of one launch, ordered by tile diagonal, then sweep, then tile:
+// every item's upstream x and y neighbours precede it.
+void build_items(int P, int G, int tx_n, int ty_n, std::vector<int> &table,
+                 std::vector<int> &index) {
+  const int S = P * G;
+  table.clear();
+  index.assign((size_t)S * tx_n * ty_n, -1);
+  for (int d = 0; d <= tx_n + ty_n - 2; ++d)
+    for (int sw = 0; sw < S; ++sw)
+      for (int tx = std::max(0, d - (ty_n - 1)); tx <= std::min(d, tx_n - 1); ++tx) {
+        const int ty = d - tx;
+        index[((size_t)sw * tx_n + tx) * ty_n + ty] = (int)table.size();
+        table.push_back((sw << 16) | (tx << 8) | ty);
+      }
+}
+
+int sweep_launches(snap_ctx *c, const void *qtot, const void *t_xs, cudaStream_t st) {
+  SweepParams p{};
+  p.nx = c->cfg.nx;
+  p.ny = c->cfg.ny;
+  p.nz = c->cfg.nz;
+  p.M = c->M;
+  p.A = c->A;
+  p.G = c->cfg.ng;
+  p.tiles_x = c->tiles_x;
+  p.tiles_y = c->tiles_y;
+  p.n_items = c->n_items;
+  p.fixup = c->cfg.fixup;
+  p.timeout_ns = c->timeout_ns;
+  p.item_table = c->d_item_table;
+  p.item_index = c->d_item_index;
+  p.qtot = qtot;
+  p.t_xs = t_xs;
+  p.phi_slots = c->d_slots;
+  p.bx = c->d_bx;
+  p.by = c->d_by;
+  p.progress = c->progress();
+  p.counter = c->counter();
+  p.error = c->error();
+  p.bt1 = c->d_bt1;
+  p.bt2 = c->d_bt2;
+  p.coef = c->d_coef;
+  for (int L = 0; L < 8 / c->P; ++L) {
+    p.o_base = L * c->P;
+    p.accumulate = L > 0;
+    SNAP_CUDA(cudaMemsetAsync(c->d_ctrl, 0, sizeof(int) * (c->n_items + 1), st));
+    cudaError_t e = c->fp32 ? launch_sweep_fp32(c->shape, p, c->grid, st)
+                            : launch_sweep_fp64(c->shape, p, c->grid, st);
+    if (e != cudaSuccess) return cuda_fail(e, "sweep launch");
+  }
+  return SNAP_OK;
+}
+
+// Reads the device error word and the violation counter (synchronises).
+int read_ctrl(snap_ctx *c, cudaStream_t st, int *violations) {
+  SNAP_CUDA(cudaMemcpyAsync(c->h_ctrl, c->error(), 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+  SNAP_CUDA(cudaStreamSynchronize(st));
+  if (c->h_ctrl[0] == DEV_ERR_TIMEOUT)
+    return fail(SNAP_ERR_DEVICE_TIMEOUT, "a sweep tile waited past its limit for an upstream tile");
+  if (c->h_ctrl[0] != 0) return fail(SNAP_ERR_CUDA, "device error word set");
+  if (violations) *violations = c->h_ctrl[1];
+  return SNAP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *snap_last_error(void) { return g_last_error.c_str(); }
+
+int snap_create(const snap_config *cfg, int device, snap_ctx **out) {
+  if (!cfg || !out) return fail(SNAP_ERR_BAD_ARG, "null argument");
+  *out = nullptr;
+  if (cfg->nx < 1 || cfg->ny < 1 || cfg->nz < 1 || cfg->nang < 1 || cfg->ng < 1 || cfg->nmom < 1 ||
+      cfg->nmom > 4 || cfg->nmat < 1 || !cfg->mu || !cfg->eta || !cfg->xi || !cfg->w || !cfg->ec)
+    return fail(SNAP_ERR_BAD_ARG, "invalid configuration");
+  if (cfg->precision != SNAP_FP64 && cfg->precision != SNAP_FP32)
+    return fail(SNAP_ERR_BAD_ARG, "unknown precision");
+  if (cfg->nx % 8 || cfg->ny % 8)
+    return fail(SNAP_ERR_UNSUPPORTED, "nx and ny must be multiples of 8");
+  if (cfg->nang > 64) return fail(SNAP_ERR_UNSUPPORTED, "at most 64 angles per octant");
+  if (cfg->nx / 8 > 255 || cfg->ny / 8 > 255)
+    return fail(SNAP_ERR_UNSUPPORTED, "at most 2040 cells along x and y");
+  if ((long long)8 * cfg->ng >= 32768) return fail(SNAP_ERR_UNSUPPORTED, "too many groups");
+
+  snap_ctx *c = new snap_ctx();
+  c->cfg = *cfg;
+  c->device = device;
+  c->fp32 = cfg->precision == SNAP_FP32;
+  c->A = cfg->nang;
+  c->M = cfg->nmom * cfg->nmom;
+  c->C = (long long)cfg->nx * cfg->ny * cfg->nz;
+  c->mu.assign(cfg->mu, cfg->mu + cfg->nang);
+  c->eta.assign(cfg->eta, cfg->eta + cfg->nang);
+  c->xi.assign(cfg->xi, cfg->xi + cfg->nang);
+  c->w.assign(cfg->w, cfg->w + cfg->nang);
+  c->ec.assign(cfg->ec, cfg->ec + (size_t)8 * c->M * cfg->nang);
+  c->cfg.mu = c->mu.data();
+  c->cfg.eta = c->eta.data();
+  c->cfg.xi = c->xi.data();
+  c->cfg.w = c->w.data();
+  c->cfg.ec = c->ec.data();
+  if (const char *t = getenv("SNAP_B200_TIMEOUT_MS")) c->timeout_ns = atoll(t) * 1000000LL;
+
+  c->shape.NT = (c->A + 7) / 8;
+  c->shape.MK = c->M == 1 ? 0 : (c->M + 3) / 4;
+  c->shape.MN = c->shape.MK == 0 ? 0 : (c->shape.MK + 1) / 2;
+  c->shape.TY = 8;
+  c->AP = 8 * c->shape.NT;
+  c->wsize = c->fp32 ? sizeof(float) : sizeof(double);
+  const bool ok = c->fp32 ? sweep_fp32_supported(c->shape) : sweep_fp64_supported(c->shape);
+  if (!ok) {
+    free_ctx(c);
+    return fail(SNAP_ERR_UNSUPPORTED, "no compiled sweep kernel for this shape");
+  }
+  c->tiles_x = cfg->nx / 8;
+  c->tiles_y = cfg->ny / c->shape.TY;
+
+  int rc;
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) {
+    free_ctx(c);
+    return cuda_fail(e, "cudaSetDevice");
+  }
+  // tables
+  if (c->fp32) {
+    std::vector<float> coef, bt1, bt2;
+    build_tables<float>(c, coef, bt1, bt2);
+    if ((rc = upload(&c->d_coef, coef)) || (rc = upload(&c->d_bt1, bt1)) ||
+        (rc = upload(&c->d_bt2, bt2))) {
+      free_ctx(c);
+      return rc;
+    }
+  } else {
+    std::vector<double> coef, bt1, bt2;
+    build_tables<double>(c, coef, bt1, bt2);
+    if ((rc = upload(&c->d_coef, coef)) || (rc = upload(&c->d_bt1, bt1)) ||
+        (rc = upload(&c->d_bt2, bt2))) {
+      free_ctx(c);
+      return rc;
+    }
+  }
+  // flux slots and tile faces: as many octants per launch as memory allows
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  const size_t budget = (size_t)(0.55 * (double)free_b);
+  const int G = cfg->ng;
+  auto scratch_for = [&](int P) {
+    const size_t items = (size_t)P * G * c->tiles_x * c->tiles_y;
+    return (size_t)P * G * c->C * c->M * c->wsize +
+           items * (size_t)cfg->nz * (c->shape.TY + 8) * c->AP * c->wsize;
+  };
+  int P = 8;
+  if (const char *pe = getenv("SNAP_B200_OCTANTS_PER_LAUNCH")) P = atoi(pe);
+  if (P != 1 && P != 2 && P != 4 && P != 8) P = 8;
+  while (P > 1 && scratch_for(P) > budget) P /= 2;
+  c->P = P;
+  std::vector<int> table, index;
+  build_items(P, G, c->tiles_x, c->tiles_y, table, index);
+  c->n_items = (int)table.size();
+  if ((rc = upload((void **)&c->d_item_table, table)) ||
+      (rc = upload((void **)&c->d_item_index, index))) {
+    free_ctx(c);
+    return rc;
+  }
+  const size_t slots_b = (size_t)P * G * c->C * c->M * c->wsize;
+  const size_t bx_b = (size_t)c->n_items * cfg->nz * c->shape.TY * c->AP * c->wsize;
+  const size_t by_b = (size_t)c->n_items * cfg->nz * 8 * c->AP * c->wsize;
+  if (cudaMalloc(&c->d_slots, slots_b) != cudaSuccess || cudaMalloc(&c->d_bx, bx_b) != cudaSuccess ||
+      cudaMalloc(&c->d_by, by_b) != cudaSuccess ||
+      cudaMalloc((void **)&c->d_ctrl, sizeof(int) * (c->n_items + 3)) != cudaSuccess) {
+    cudaGetLastError();
+    free_ctx(c);
+    return fail(SNAP_ERR_OOM, "cannot allocate sweep scratch");
+  }
+  c->scratch_bytes = slots_b + bx_b + by_b + sizeof(int) * (c->n_items + 3);
+  if (cudaMemset(c->d_ctrl, 0, sizeof(int) * (c->n_items + 3)) != cudaSuccess ||
+      cudaMallocHost((void **)&c->h_ctrl, 4 * sizeof(int)) != cudaSuccess ||
+      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+    free_ctx(c);
+    return fail(SNAP_ERR_CUDA, "context setup failed");
+  }
+  int blocks = 0, sms = 0;
+  size_t smem = 0;
+  e = c->fp32 ? sweep_fp32_occupancy(c->shape, &blocks, &smem)
+              : sweep_fp64_occupancy(c->shape, &blocks, &smem);
+  if (e != cudaSuccess || blocks < 1) {
+    free_ctx(c);
+    return fail(SNAP_ERR_UNSUPPORTED, "sweep kernel does not fit on the device");
+  }
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  c->grid = std::min(blocks * sms, c->n_items);
+  if (const char *ge = getenv("SNAP_B200_GRID")) c->grid = std::max(1, std::min(atoi(ge), c->grid));
+  *out = c;
+  return SNAP_OK;
+}
+
+int snap_destroy(snap_ctx *ctx) {
+  free_ctx(ctx);
+  return SNAP_OK;
+}
+
+size_t snap_scratch_bytes(const snap_ctx *ctx) { return ctx ? ctx->scratch_bytes : 0; }
+
+int snap_expand_xs(snap_ctx *c, const double *sig, const int32_t *mat, double *xs, void *stream) {
+  if (!c || !sig || !mat || !xs) return fail(SNAP_ERR_BAD_ARG, "null argument");
+  SNAP_CUDA(k_expand_xs(sig, mat, xs, c->cfg.ng, c->cfg.nmat, c->C, (cudaStream_t)stream));
+  return SNAP_OK;
+}
+
+int snap_expand_scattering_xs(snap_ctx *c, const double *slgg, const int32_t *mat, double *s_xs,
+                              void *stream) {
+  if (!c || !slgg || !mat || !s_xs) return fail(SNAP_ERR_BAD_ARG, "null argument");
+  SNAP_CUDA(k_expand_scat(slgg, mat, s_xs, c->cfg.ng, c->cfg.nmat, c->cfg.nmom, c->C,
+                          (cudaStream_t)stream));
+  return SNAP_OK;
+}
+
+int snap_calc_outer_source(snap_ctx *c, const double *qi, const double *slgg, const int32_t *mat,
+                           const double *flux, double *q2grp, void *stream) {
+  if (!c || !qi || !slgg || !mat || !flux || !q2grp) return fail(SNAP_ERR_BAD_ARG, "null argument");
+  SNAP_CUDA(k_outer_source(qi, slgg, mat, flux, q2grp, c->cfg.ng, c->cfg.nmat, c->cfg.nmom, c->M,
+                           c->C, (cudaStream_t)stream));
+  return SNAP_OK;
+}
+
+int snap_calc_inner_source(snap_ctx *c, const double *s_xs, const double *q2grp,
+                           const double *flux, void *qtot, void *stream) {
+  if (!c || !s_xs || !q2grp || !flux || !qtot) return fail(SNAP_ERR_BAD_ARG, "null argument");
+  SNAP_CUDA(k_inner_source(s_xs, q2grp, flux, qtot, c->fp32, c->cfg.ng, c->cfg.nmom, c->M, c->C,
+                           (cudaStream_t)stream));
+  return SNAP_OK;
+}
+
+int snap_sweep(snap_ctx *c, const void *qtot, const void *t_xs, void *flux, void *stream) {
+  if (!c || !qtot || !t_xs || !flux) return fail(SNAP_ERR_BAD_ARG, "null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  SNAP_CUDA(cudaMemsetAsync(c->error(), 0, 2 * sizeof(int), st));
+  int rc = sweep_launches(c, qtot, t_xs, st);
+  if (rc) return rc;
+  SNAP_CUDA(k_reduce_slots(c->d_slots, c->P, c->fp32, flux, c->fp32, nullptr, c->cfg.ng, c->M,
+                           c->C, 0, 0.0, nullptr, st));
+  return read_ctrl(c, st, nullptr);
+}
+
+int snap_test_convergence(snap_ctx *c, int kind, const double *flux, const double *prev,
+                          double epsi, int *converged, void *stream) {
+  if (!c || !flux || !prev || !converged || (kind != 0 && kind != 1))
+    return fail(SNAP_ERR_BAD_ARG, "bad argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  SNAP_CUDA(cudaMemsetAsync(c->error(), 0, 2 * sizeof(int), st));
+  SNAP_CUDA(k_count_violations(flux, prev, c->M, (long long)c->cfg.ng * c->C, epsi,
+                               c->violations(), st));
+  int v = 0;
+  int rc = read_ctrl(c, st, &v);
+  if (rc) return rc;
+  *converged = v == 0;
+  return SNAP_OK;
+}
+
+int snap_transport_solve(snap_ctx *c, const int32_t *mat, const double *qi, const double *sigt,
+                         const double *slgg, const double *sigt_scale, double *flux,
+                         snap_solve_info *info, void *stream) {
+  if (!c || !mat || !qi || !sigt || !slgg || !flux || !info)
+    return fail(SNAP_ERR_BAD_ARG, "null argument");
+  if (info->iitm < 1 || info->oitm < 1 || !(info->epsi > 0.0))
+    return fail(SNAP_ERR_BAD_ARG, "iitm, oitm and epsi must be positive");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int G = c->cfg.ng, M = c->M, nmom = c->cfg.nmom;
+  const long long C = c->C, n = (long long)G * C;
+  double *t_xs64 = nullptr, *s_xs = nullptr, *q2grp = nullptr, *fpo = nullptr;
+  void *qtot = nullptr, *t_xs_sw = nullptr;
+  auto cleanup = [&]() {
+    cudaFree(t_xs64);
+    cudaFree(s_xs);
+    cudaFree(q2grp);
+    cudaFree(fpo);
+    cudaFree(qtot);
+    if (t_xs_sw != t_xs64) cudaFree(t_xs_sw);
+  };
+  if (cudaMalloc(&t_xs64, sizeof(double) * n) != cudaSuccess ||
+      cudaMalloc(&s_xs, sizeof(double) * n * nmom) != cudaSuccess ||
+      cudaMalloc(&q2grp, sizeof(double) * n * M) != cudaSuccess ||
+      cudaMalloc(&fpo, sizeof(double) * n * M) != cudaSuccess ||
+      cudaMalloc(&qtot, c->wsize * n * M) != cudaSuccess) {
+    cudaGetLastError();
+    cleanup();
+    return fail(SNAP_ERR_OOM, "cannot allocate solve arrays");
+  }
+  t_xs_sw = t_xs64;
+  int rc = SNAP_OK;
+#define STEP(x)                 \
+  do {                          \
+    cudaError_t e_ = (x);       \
+    if (e_ != cudaSuccess) {    \
+      rc = cuda_fail(e_, #x);   \
+      goto done;                \
+    }                           \
+  } while (0)
+  {
+    info->inner_total = info->outer_total = info->converged = 0;
+    info->sweep_ms = info->total_ms = 0.0;
+    float ms = 0.0f;
+    STEP(cudaMemsetAsync(c->error(), 0, 2 * sizeof(int), st));
+    STEP(cudaEventRecord(c->ev0, st));
+    // per time step expansion (snap.cc:419-450)
+    STEP(k_expand_xs(sigt, mat, t_xs64, G, c->cfg.nmat, C, st));
+    if (sigt_scale) STEP(k_scale_xs(t_xs64, sigt_scale, G, C, st));
+    STEP(k_expand_scat(slgg, mat, s_xs, G, c->cfg.nmat, nmom, C, st));
+    if (c->fp32) {
+      if (cudaMalloc(&t_xs_sw, sizeof(float) * n) != cudaSuccess) {
+        t_xs_sw = t_xs64;
+        rc = fail(SNAP_ERR_OOM, "cannot allocate t_xs");
+        goto done;
+      }
+      STEP(k_to_f32(t_xs64, (float *)t_xs_sw, n, st));
+    }
+    STEP(cudaMemsetAsync(flux, 0, sizeof(double) * n * M, st));   // snap.cc:313-316
+    for (int o = 0; o < info->oitm; ++o) {
+      STEP(k_outer_source(qi, slgg, mat, flux, q2grp, G, c->cfg.nmat, nmom, M, C, st));
+      STEP(k_copy_moment0(flux, fpo, M, n, st));                   // save_fluxes -> flux0po
+      bool inner_conv = false;
+      int inners = 0;
+      for (int i = 0; i < info->iitm; ++i) {
+        STEP(k_inner_source(s_xs, q2grp, flux, qtot, c->fp32, G, nmom, M, C, st));
+        STEP(cudaMemsetAsync(c->violations(), 0, sizeof(int), st));
+        rc = sweep_launches(c, qtot, t_xs_sw, st);
+        if (rc) goto done;
+        // flux = sum of octant slots, inner test against the previous flux
+        STEP(k_reduce_slots(c->d_slots, c->P, c->fp32, flux, 0, flux, G, M, C, 1, info->epsi,
+                            c->violations(), st));
+        int v = 0;
+        rc = read_ctrl(c, st, &v);
+        if (rc) goto done;
+        ++inners;
+        ++info->inner_total;
+        inner_conv = v == 0;
+        if (inner_conv) break;
+      }
+      if (o < 1024) info->inners_per_outer[o] = inners;
+      ++info->outer_total;
+      if (o == 0) continue;                                        // snap.cc:521-522
+      if (inner_conv) {
+        STEP(cudaMemsetAsync(c->violations(), 0, sizeof(int), st));
+        STEP(k_count_violations(flux, fpo, M, n, 100.0 * info->epsi, c->violations(), st));
+        int v = 0;
+        rc = read_ctrl(c, st, &v);
+        if (rc) goto done;
+        if (v == 0) {
+          info->converged = 1;
+          break;
+        }
+      }
+    }
+    STEP(cudaEventRecord(c->ev1, st));
+    STEP(cudaEventSynchronize(c->ev1));
+    STEP(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    info->total_ms = ms;
+  }
+done:
+  cleanup();
+#undef STEP
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,165 @@
+"""Host-side mirror of the reference's task-level interface on the solve path.
+
+Each method of :class:`Snap` corresponds to one of the reference's logical
+tasks and calls the matching C ABI entry point (include/snap_b200.h) on CUDA
+tensors owned by the caller.  Names follow the reference's task classes:
+
+=============================  ==============================================
+reference task                 method
+=============================  ==============================================
+ExpandCrossSection             ``expand_cross_section`` (expxs.cc:25-160)
+ExpandScatteringCrossSection   ``expand_scattering_cross_section``
+                               (expxs.cc:163-290)
+CalcOuterSource                ``calc_outer_source`` (outer.cc:26-284)
+CalcInnerSource                ``calc_inner_source`` (inner.cc:27-215)
+MiniKBATask (8 octants x G)    ``mini_kba_sweep`` (sweep.cc:28-129,
+                               snap.cc:849-887)
+TestInnerConvergence           ``test_inner_convergence`` (inner.cc:218-367)
+TestOuterConvergence           ``test_outer_convergence`` (outer.cc:287-451)
+Snap::transport_solve          ``transport_solve`` (snap.cc:225-568)
+=============================  ==============================================
+
+Torch is used for device memory and the current stream only.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import abi
+from .problem import Deck, quadrature
+
+
+def _ptr(t: torch.Tensor) -> int:
+    assert t.is_cuda and t.is_contiguous()
+    return t.data_ptr()
+
+
+def _stream() -> int:
+    return torch.cuda.current_stream().cuda_stream
+
+
+class Snap:
+    """One context (quadrature tables + sweep scratch) for a deck on one GPU."""
+
+    def __init__(self, deck: Deck, precision: str = "fp64", device: int = 0):
+        self.lib = abi.load()
+        self.deck = deck
+        self.device = torch.device("cuda", device)
+        self.precision = precision
+        self.sweep_dtype = torch.float64 if precision == "fp64" else torch.float32
+        mu, eta, xi, w, ec = quadrature(deck.nang, deck.nmom)
+        self._host = [np.ascontiguousarray(a, dtype=np.float64) for a in (mu, eta, xi, w, ec)]
+        dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))  # noqa: E731
+        cfg = abi.SnapConfig(
+            deck.nx, deck.ny, deck.nz, deck.nang, deck.ng, deck.nmom, 2, int(deck.fixup),
+            abi.SNAP_FP64 if precision == "fp64" else abi.SNAP_FP32,
+            2.0 * deck.nx / deck.lx, 2.0 * deck.ny / deck.ly, 2.0 * deck.nz / deck.lz,
+            *(dp(a) for a in self._host))
+        handle = C.c_void_p()
+        with torch.cuda.device(self.device):
+            abi.check(self.lib.snap_create(C.byref(cfg), device, C.byref(handle)))
+        self.handle = handle
+
+    def close(self):
+        if self.handle:
+            self.lib.snap_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def scratch_bytes(self) -> int:
+        return int(self.lib.snap_scratch_bytes(self.handle))
+
+    # ---- allocation helpers -------------------------------------------------
+    def _empty(self, *shape, dtype=torch.float64):
+        return torch.empty(*shape, dtype=dtype, device=self.device)
+
+    @property
+    def C(self) -> int:
+        return self.deck.cells
+
+    # ---- task-level operations ----------------------------------------------
+    def expand_cross_section(self, sig: torch.Tensor, mat: torch.Tensor) -> torch.Tensor:
+        xs = self._empty(self.deck.ng, self.C)
+        abi.check(self.lib.snap_expand_xs(self.handle, _ptr(sig), _ptr(mat), _ptr(xs), _stream()))
+        return xs
+
+    def expand_scattering_cross_section(self, slgg, mat) -> torch.Tensor:
+        s_xs = self._empty(self.deck.ng, self.C, self.deck.nmom)
+        abi.check(self.lib.snap_expand_scattering_xs(self.handle, _ptr(slgg), _ptr(mat),
+                                                     _ptr(s_xs), _stream()))
+        return s_xs
+
+    def calc_outer_source(self, qi, slgg, mat, flux) -> torch.Tensor:
+        q2 = self._empty(self.deck.ng, self.C, self.deck.cmom)
+        abi.check(self.lib.snap_calc_outer_source(self.handle, _ptr(qi), _ptr(slgg), _ptr(mat),
+                                                  _ptr(flux), _ptr(q2), _stream()))
+        return q2
+
+    def calc_inner_source(self, s_xs, q2grp, flux) -> torch.Tensor:
+        qtot = self._empty(self.deck.ng, self.C, self.deck.cmom, dtype=self.sweep_dtype)
+        abi.check(self.lib.snap_calc_inner_source(self.handle, _ptr(s_xs), _ptr(q2grp),
+                                                  _ptr(flux), _ptr(qtot), _stream()))
+        return qtot
+
+    def mini_kba_sweep(self, qtot, t_xs) -> torch.Tensor:
+        flux = self._empty(self.deck.ng, self.C, self.deck.cmom, dtype=self.sweep_dtype)
+        abi.check(self.lib.snap_sweep(self.handle, _ptr(qtot), _ptr(t_xs), _ptr(flux), _stream()))
+        return flux
+
+    def _test(self, kind, flux, prev, epsi) -> bool:
+        conv = C.c_int(0)
+        abi.check(self.lib.snap_test_convergence(self.handle, kind, _ptr(flux), _ptr(prev),
+                                                 C.c_double(epsi), C.byref(conv), _stream()))
+        return bool(conv.value)
+
+    def test_inner_convergence(self, flux, flux_pi) -> bool:
+        return self._test(0, flux, flux_pi, self.deck.epsi)
+
+    def test_outer_convergence(self, flux, flux_po, inner_converged: bool) -> bool:
+        if not inner_converged:       # outer.cc:361-365
+            return False
+        return self._test(1, flux, flux_po, 100.0 * self.deck.epsi)
+
+    # ---- the solve loop ----------------------------------------------------
+    def device_problem(self, prob: dict) -> dict:
+        dev = self.device
+        out = dict(
+            mat=torch.as_tensor(prob["mat"], device=dev),
+            qi=torch.as_tensor(np.ascontiguousarray(prob["qi"]), device=dev),
+            sigt=torch.as_tensor(np.ascontiguousarray(prob["sigt"]), device=dev),
+            slgg=torch.as_tensor(np.ascontiguousarray(prob["slgg"]), device=dev),
+        )
+        if "sigt_scale" in prob:
+            out["sigt_scale"] = torch.as_tensor(prob["sigt_scale"], device=dev)
+        return out
+
+    def transport_solve(self, dprob: dict, flux: torch.Tensor | None = None,
+                        epsi=None, iitm=None, oitm=None):
+        """Runs the whole steady-state solve on the device.  Returns the flux
+        moments [G, C, cmom] (float64) and the iteration record."""
+        d = self.deck
+        if flux is None:
+            flux = self._empty(d.ng, self.C, d.cmom)
+        info = abi.SnapSolveInfo()
+        info.epsi = d.epsi if epsi is None else epsi
+        info.iitm = d.iitm if iitm is None else iitm
+        info.oitm = d.oitm if oitm is None else oitm
+        scale = dprob.get("sigt_scale")
+        abi.check(self.lib.snap_transport_solve(
+            self.handle, _ptr(dprob["mat"]), _ptr(dprob["qi"]), _ptr(dprob["sigt"]),
+            _ptr(dprob["slgg"]), _ptr(scale) if scale is not None else None, _ptr(flux),
+            C.byref(info), _stream()))
+        rec = dict(inner_total=info.inner_total, outer_total=info.outer_total,
+                   converged=bool(info.converged),
+                   inners_per_outer=list(info.inners_per_outer[:info.outer_total]),
+                   total_ms=info.total_ms)
+        return flux, rec

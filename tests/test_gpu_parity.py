@@ -1,0 +1,236 @@
+"""GPU parity: the CUDA path through the C ABI against the reference's golden
+vectors and the CPU oracle.  FP64 tolerance: 1e-12 relative in scalar flux
+(higher moments: 1e-12 of the moment's largest magnitude)."""
+import os
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = [
+    pytest.mark.gpu,
+    pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA device"),
+]
+
+from oracle.bindings import Oracle  # noqa: E402
+from snap_b200 import problem as P  # noqa: E402
+
+TOL = 1e-12
+
+
+def rel_err(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300)))
+
+
+def moment_err(a, b):
+    """max over moments of max|a-b| / max|b| for that moment."""
+    a = np.asarray(a).reshape(-1, a.shape[-1])
+    b = np.asarray(b).reshape(-1, b.shape[-1])
+    scale = np.maximum(np.abs(b).max(axis=0), 1e-300)
+    return float((np.abs(a - b).max(axis=0) / scale).max())
+
+
+def snap_ctx(deck, **env):
+    from snap_b200.solver import Snap
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update({k: str(v) for k, v in env.items()})
+    try:
+        return Snap(deck)
+    finally:
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+
+
+def dev(a, dtype=None):
+    return torch.as_tensor(np.ascontiguousarray(a), device="cuda")
+
+
+def random_qtot(deck, seed):
+    rng = np.random.default_rng(seed)
+    q = rng.uniform(0.0, 1.0, size=(deck.ng, deck.cells, deck.cmom))
+    if deck.cmom > 1:
+        q[..., 1:] = rng.uniform(-0.2, 0.2, size=q[..., 1:].shape)
+    return q
+
+
+@pytest.fixture(scope="module")
+def golden(golden_dir):
+    return {k: np.load(golden_dir / f"{k}_ref.npz") for k in ("deck1", "deck2p")}
+
+
+# ---------------------------------------------------------------- task level
+@pytest.mark.parametrize("d", [P.deck(1), P.Deck(16, 8, 8, nang=12, ng=3, nmom=3)])
+def test_expand_cross_sections(d):
+    prob = P.make_problem(d)
+    snap = snap_ctx(d)
+    t_xs = snap.expand_cross_section(dev(prob["sigt"]), dev(prob["mat"])).cpu().numpy()
+    s_xs = snap.expand_scattering_cross_section(dev(prob["slgg"]), dev(prob["mat"])).cpu().numpy()
+    ot, os_ = Oracle(d).expand(prob)
+    assert np.array_equal(t_xs, ot)
+    assert np.array_equal(s_xs, os_)
+
+
+@pytest.mark.parametrize("d", [P.deck(1), P.Deck(16, 8, 8, nang=12, ng=5, nmom=4)])
+def test_outer_and_inner_source(d):
+    prob = P.make_problem(d)
+    o = Oracle(d)
+    _, s_xs = o.expand(prob)
+    flux = random_qtot(d, 7)
+    snap = snap_ctx(d)
+    q2 = snap.calc_outer_source(dev(prob["qi"]), dev(prob["slgg"]), dev(prob["mat"]), dev(flux))
+    q2_ref = o.outer_source(prob, flux)
+    assert moment_err(q2.cpu().numpy(), q2_ref) < 1e-14
+    qtot = snap.calc_inner_source(dev(s_xs), q2, dev(flux)).cpu().numpy()
+    assert moment_err(qtot, o.inner_source(s_xs, q2_ref, flux)) < 1e-14
+
+
+# ---------------------------------------------------------------- sweep
+SWEEP_DECKS = [
+    P.deck(1),                                           # A=10 (2 angle tiles), one moment
+    P.Deck(16, 16, 16, nang=36, ng=3, nmom=4),           # deck-2 angular shape, 16 moments
+    P.Deck(16, 8, 24, nang=24, ng=2, nmom=2),            # adjoint-deck shape, 4 moments
+    P.Deck(8, 16, 8, nang=48, ng=2, nmom=3),             # deck-3/5 angles, 9 moments
+    P.Deck(8, 8, 5, nang=3, ng=1, nmom=1),               # tiny: one tile, ragged angle tile
+]
+
+
+@pytest.mark.parametrize("d", SWEEP_DECKS, ids=lambda d: f"{d.nx}x{d.ny}x{d.nz}_A{d.nang}_M{d.cmom}")
+def test_sweep_matches_oracle(d):
+    prob = P.make_problem(d)
+    o = Oracle(d)
+    t_xs, _ = o.expand(prob)
+    qtot = random_qtot(d, 11)
+    ref = o.sweep(qtot, t_xs)
+    snap = snap_ctx(d)
+    got = snap.mini_kba_sweep(dev(qtot), dev(t_xs)).cpu().numpy()
+    assert rel_err(got[..., 0], ref[..., 0]) < TOL
+    assert moment_err(got, ref) < TOL
+
+
+@pytest.mark.parametrize("env", [dict(SNAP_B200_OCTANTS_PER_LAUNCH=2),
+                                 dict(SNAP_B200_OCTANTS_PER_LAUNCH=1),
+                                 dict(SNAP_B200_GRID=1),
+                                 dict(SNAP_B200_GRID=3, SNAP_B200_OCTANTS_PER_LAUNCH=4)],
+                         ids=["P2", "P1", "grid1", "grid3_P4"])
+def test_sweep_launch_plans(env):
+    """Fewer octants per launch (slot accumulation) and tiny persistent grids
+    (a single CTA walks every item in queue order) give the same flux."""
+    d = P.Deck(16, 16, 8, nang=12, ng=2, nmom=2)
+    prob = P.make_problem(d)
+    o = Oracle(d)
+    t_xs, _ = o.expand(prob)
+    qtot = random_qtot(d, 3)
+    ref = o.sweep(qtot, t_xs)
+    got = snap_ctx(d, **env).mini_kba_sweep(dev(qtot), dev(t_xs)).cpu().numpy()
+    assert moment_err(got, ref) < TOL
+
+
+def thick_point_source(d):
+    prob = P.make_problem(d)
+    prob["sigt"] = prob["sigt"] * 40.0
+    prob["slgg"] = prob["slgg"] * 40.0
+    prob["qi"][:] = 0.0
+    c = (d.nz // 2 * d.ny + d.ny // 2) * d.nx + d.nx // 2
+    prob["qi"][:, c] = 100.0
+    return prob
+
+
+@pytest.mark.parametrize("nmom", [1, 2])
+def test_sweep_fixup_heavy(nmom):
+    """Optically thick cells around a point source: most cells take the
+    negative-flux fixup path."""
+    d = P.Deck(16, 16, 8, nang=10, ng=2, nmom=nmom)
+    prob = thick_point_source(d)
+    o = Oracle(d)
+    t_xs, s_xs = o.expand(prob)
+    q2 = o.outer_source(prob, np.zeros((d.ng, d.cells, d.cmom)))
+    qtot = o.inner_source(s_xs, q2, np.zeros((d.ng, d.cells, d.cmom)))
+    ref = o.sweep(qtot, t_xs)
+    nofix = Oracle(P.Deck(**{**d.__dict__, "fixup": False})).sweep(qtot, t_xs)
+    assert rel_err(nofix[..., 0], ref[..., 0]) > 1e-3      # the fixup mattered
+    got = snap_ctx(d).mini_kba_sweep(dev(qtot), dev(t_xs)).cpu().numpy()
+    assert rel_err(got[..., 0], ref[..., 0]) < TOL
+    assert moment_err(got, ref) < TOL
+
+
+def test_convergence_tests():
+    d = P.Deck(8, 8, 8, nang=2, ng=2, nmom=2)
+    snap = snap_ctx(d)
+    rng = np.random.default_rng(5)
+    prev = rng.uniform(0.5, 1.0, size=(d.ng, d.cells, d.cmom))
+    flux = prev * (1 + 0.5e-4)
+    assert snap.test_inner_convergence(dev(flux), dev(prev))
+    flux[1, 17, 0] = prev[1, 17, 0] * 1.01
+    assert not snap.test_inner_convergence(dev(flux), dev(prev))
+    assert snap.test_outer_convergence(dev(flux), dev(prev), True) is False
+    flux[1, 17, 0] = prev[1, 17, 0] * (1 + 0.9e-2)   # within 100 eps
+    assert snap.test_outer_convergence(dev(flux), dev(prev), True)
+    assert snap.test_outer_convergence(dev(flux), dev(prev), False) is False
+    prev[0, 3, 0] = 0.0                                # |prev| < 1e-12: tests |flux|
+    flux[0, 3, 0] = 5e-5
+    assert snap.test_inner_convergence(dev(flux), dev(prev)) is False  # flux[1,17] still off
+    flux[1, 17, 0] = prev[1, 17, 0]
+    assert snap.test_inner_convergence(dev(flux), dev(prev))
+
+
+# ---------------------------------------------------------------- full solves
+def test_solve_deck1_matches_reference(golden):
+    """16^3, A=10, G=4: every cell and group against the reference's own task
+    bodies, and the same iteration record."""
+    g = golden["deck1"]
+    d = P.deck(1)
+    snap = snap_ctx(d)
+    flux, rec = snap.transport_solve(snap.device_problem(P.make_problem(d)))
+    assert rel_err(flux[..., 0].cpu().numpy(), g["flux0"]) < TOL
+    assert rec["inner_total"] == int(g["inner_total"])
+    assert rec["outer_total"] == int(g["outer_total"])
+    assert rec["converged"] == bool(g["converged"])
+    assert rec["inners_per_outer"] == list(g["inners_per_outer"])
+
+
+def test_solve_deck2p_matches_reference(golden):
+    """64^3, A=36, G=32, nmom=1 (deck 2 at one moment): the reference's
+    converged scalar flux at 4096 seeded samples, per-group sums and maxima,
+    and the iteration record."""
+    g = golden["deck2p"]
+    d = P.deck(2, nmom=1)
+    snap = snap_ctx(d)
+    flux, rec = snap.transport_solve(snap.device_problem(P.make_problem(d)))
+    phi = flux[..., 0].cpu().numpy()
+    assert rel_err(phi[g["sample_g"], g["sample_c"]], g["sample_flux0"]) < TOL
+    assert rel_err(phi.sum(axis=1), g["group_sum"]) < TOL
+    assert rel_err(phi.max(axis=1), g["group_max"]) < TOL
+    assert rec["inner_total"] == int(g["inner_total"])
+    assert rec["outer_total"] == int(g["outer_total"])
+    assert rec["inners_per_outer"] == list(g["inners_per_outer"])
+
+
+def test_solve_multimoment_matches_oracle():
+    d = P.Deck(16, 16, 16, nang=12, ng=4, nmom=4, epsi=1e-6, iitm=3, oitm=4)
+    prob = P.make_problem(d)
+    ref, rref = Oracle(d).solve(prob)
+    snap = snap_ctx(d)
+    flux, rec = snap.transport_solve(snap.device_problem(prob))
+    got = flux.cpu().numpy()
+    assert rel_err(got[..., 0], ref[..., 0]) < TOL
+    assert moment_err(got, ref) < TOL
+    assert rec["inners_per_outer"] == rref["inners_per_outer"]
+
+
+def test_solve_deck2_full_size_properties():
+    """Deck 2 at full size (64^3, A=36, G=32, nmom=4): converges, stays finite
+    and positive, and keeps the problem's three mirror symmetries to 1e-12."""
+    d = P.deck(2)
+    snap = snap_ctx(d)
+    flux, rec = snap.transport_solve(snap.device_problem(P.make_problem(d)))
+    assert rec["converged"]
+    phi = flux[..., 0].reshape(d.ng, d.nz, d.ny, d.nx)
+    assert torch.isfinite(flux).all()
+    assert (phi > 0).all()
+    for dim in (1, 2, 3):
+        assert rel_err(phi.flip(dim).cpu().numpy(), phi.cpu().numpy()) < TOL
