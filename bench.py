@@ -1,0 +1,355 @@
+#!/usr/bin/env python
+"""Grind-time benchmark of the steady-state solve path on deck 2.
+
+Workload (deck 2): 64^3 cells on the unit cube, 36 angles per octant (288),
+32 groups, nmom = 4 (16 flux moments), FP64, centre material-2 block with a
+unit source, fixup on.  Inputs are generated on the host with the deck's
+cross-section rule (synthetic, seeded; there is no external data set).
+
+A step is one inner iteration on device-resident data (inner source, the
+8-octant x 32-group sweep, octant sum and inner convergence test).  The metric
+is grind time = step time / (cells x 8 x angles x groups), in ns; lower is
+better.  qtot alone is 1.07 GB per step, far larger than the 126 MB L2, so no
+L2 flush is needed between steps.
+
+  value   device-resident grind time (CUDA events, max over ranks)
+  e2e     grind time of whole solves through the public C ABI
+          (snap_transport_solve) from pinned host buffers, host->device copies
+          of the deck and the device->host copy of the flux inside the timed
+          region, per inner iteration executed
+  roofline  the sweep kernel: algorithmic bytes (3*cmom+1)*8/angles per unit
+          x units per launch / CUDA-event duration, against the measured HBM
+          copy bandwidth
+  cpu_baseline  the reference's own CPU task bodies (oracle/_ref) on the host
+          cores, bounded sample
+
+--impl reference times the reference's CPU path alone (rank 0 only).
+Multi-GPU (torchrun): each rank owns a 32-group shard (weak scaling); the
+only exchange in a step is the convergence AND (NCCL all-reduce of one int).
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "legion-snap_b200"))
+
+METRIC = "grind time ns/(cell*angle*group), FP64 inner iteration"
+UNIT = "ns"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["snap", "reference"], default="snap")
+    ap.add_argument("--e2e-solves", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-inners", type=int, default=2)
+    ap.add_argument("--groups", type=int, default=None,
+                    help="override deck 2's 32 groups (small cases for profiling only)")
+    return ap.parse_args()
+
+
+GROUPS = None
+
+
+def deck2():
+    from snap_b200 import problem as P
+    return P.deck(2) if GROUPS is None else P.deck(2, ng=GROUPS)
+
+
+def workload_config(d, precision="fp64"):
+    return {
+        "workload": "deck 2: 64^3 cells, 36 angles/octant, 32 groups, nmom=4 (16 moments), "
+                    "steady-state fixed source, fixup on",
+        "cells": d.cells, "angles_per_octant": d.nang, "groups": d.ng, "nmom": d.nmom,
+        "cmom": d.cmom, "precision": precision,
+        "step": "one inner iteration: inner source + sweep of 8 octants x all groups + "
+                "octant sum + inner convergence test",
+        "units_per_step": d.units_per_sweep,
+        "l2": "inputs larger than L2 (qtot 1.07 GB per step), no flush",
+        "parallelism": "group shards per rank (weak)",
+    }
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        j = json.loads(p.read_text())
+        return float(j["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic(name: str):
+    """dram bytes per launch recorded in profiles/<name>.md (line
+    'traffic_bytes_per_launch: N'), or None."""
+    p = ROOT / "profiles" / f"{name}.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.strip().startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.2)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        rows = []
+        for line in open(self.file.name):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append(dict(sm=float(parts[1]), smax=float(parts[2]),
+                                 hw=parts[5], hwt=parts[6], swt=parts[7], pcap=parts[8]))
+            except ValueError:
+                continue
+        os.unlink(self.file.name)
+        if not rows:
+            return None
+        reasons = set()
+        for r in rows:
+            for key, name in (("hw", "hw_slowdown"), ("hwt", "hw_thermal_slowdown"),
+                              ("swt", "sw_thermal_slowdown"), ("pcap", "sw_power_cap")):
+                if r[key].lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(r["sm"] for r in rows),
+                "sm_max_mhz": max(r["smax"] for r in rows),
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def cpu_reference_sample(d, inners: int):
+    """The reference's own CPU task bodies on deck 2's mesh, angles and groups
+    at nmom = 1 (its nmom > 1 sweep path dereferences an unbound flux-moment
+    accessor), all host threads, `inners` inner iterations."""
+    from oracle.bindings import RefSnap
+    from snap_b200 import problem as P
+    if not RefSnap.available():
+        return None
+    dd = P.Deck(**{**d.__dict__, "nmom": 1})
+    ref = RefSnap(dd)
+    prob = P.make_problem(dd)
+    threads = os.cpu_count() or 1
+    _, rec = ref.solve(prob, nthreads=threads, max_inners=inners)
+    grind = rec["seconds"] * 1e9 / (dd.units_per_sweep * rec["inner_total"])
+    return {"value": grind, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"reference CPU task bodies (variant {rec['variant']}: "
+                      f"{['scalar', 'SSE', 'AVX'][rec['variant']]}), deck 2 mesh/angles/groups "
+                      f"at nmom=1, {rec['inner_total']} inner iterations incl. one outer source, "
+                      f"{threads} threads",
+            "sweep_only_ns": rec["sweep_seconds"] * 1e9 / (dd.units_per_sweep * rec["inner_total"])}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    d = deck2()
+    vals = []
+    sample = None
+    for i in range(args.warmup + args.steps):
+        s = cpu_reference_sample(d, 1)
+        if s is None:
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "reference CPU build oracle/_ref/libsnapref.so not present"}))
+            return 0
+        if i >= args.warmup:
+            vals.append(s["value"])
+            sample = s
+    value = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": value * d.units_per_sweep / 1e6, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(d, "fp64 (reference CPU at nmom=1)"),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": sample["cores"],
+                         "kind": "reference", "sample": sample["sample"]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_snap(args):
+    import torch
+    import torch.distributed as dist
+
+    from snap_b200 import problem as P
+    from snap_b200.solver import Snap
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    d = deck2()
+    snap = Snap(d, device=local)
+    prob = P.make_problem(d)
+    dp = snap.device_problem(prob)
+    t_xs = snap.expand_cross_section(dp["sigt"], dp["mat"])
+    s_xs = snap.expand_scattering_cross_section(dp["slgg"], dp["mat"])
+    flux = torch.zeros(d.ng, d.cells, d.cmom, dtype=torch.float64, device="cuda")
+    q2grp = snap.calc_outer_source(dp["qi"], dp["slgg"], dp["mat"], flux)
+    qtot = torch.empty(d.ng, d.cells, d.cmom, dtype=torch.float64, device="cuda")
+
+    def step():
+        conv = snap.inner_iteration(s_xs, q2grp, t_xs, flux, qtot)
+        if world > 1:   # global convergence = AND over the group shards
+            flag = torch.tensor([0 if conv else 1], dtype=torch.int32, device="cuda")
+            dist.all_reduce(flag)
+            conv = int(flag.item()) == 0
+        return conv
+
+    for _ in range(args.warmup):
+        step()
+    clocks = ClockSampler(local)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    snap.timing(reset=True)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        step()
+    ev1.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    tm = snap.timing()
+    ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms = float(ms_t.item())
+    ms_per_step = ms / args.steps
+    units_step = d.units_per_sweep * world
+    value = ms_per_step * 1e6 / units_step
+
+    # roofline of the sweep kernel
+    sweep_ms = tm["sweep_ms"] / max(tm["sweep_calls"], 1)
+    bytes_unit = (3 * d.cmom + 1) * 8 / d.nang
+    algo = bytes_unit * d.units_per_sweep
+    achieved = algo / (sweep_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = ncu_traffic("sweep_fp64_deck2")
+
+    # end to end: whole solves through the C ABI from pinned host memory
+    host = {k: torch.as_tensor(v).pin_memory() for k, v in
+            (("mat", prob["mat"]), ("qi", prob["qi"]), ("sigt", prob["sigt"]),
+             ("slgg", prob["slgg"]))}
+    flux_host = torch.empty(d.ng, d.cells, d.cmom, dtype=torch.float64).pin_memory()
+    h2d = sum(t.numel() * t.element_size() for t in host.values())
+    d2h = flux_host.numel() * flux_host.element_size()
+    e2e_vals = []
+    for _ in range(args.e2e_solves):
+        dev = {k: torch.empty_like(v, device="cuda") for k, v in host.items()}
+        out = torch.empty(d.ng, d.cells, d.cmom, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for k in dev:
+            dev[k].copy_(host[k], non_blocking=True)
+        _, rec = snap.transport_solve(dev, flux=out)
+        flux_host.copy_(out, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        e2e_vals.append(e0.elapsed_time(e1) * 1e6 / (d.units_per_sweep * rec["inner_total"]))
+    e2e_t = torch.tensor([statistics.mean(e2e_vals) if e2e_vals else float("nan")],
+                         dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e = float(e2e_t.item()) / world
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (deck-2 rule, generated on the host)",
+        "config": workload_config(d),
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "step": "one whole solve (snap_transport_solve), per inner iteration executed",
+                "inner_iterations": rec["inner_total"] if e2e_vals else 0},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "kernel": "sweep_fp64_kernel", "peak_source": f"{peak_kind} hbm_gbs",
+                     "bytes_per_unit": bytes_unit, "sweep_ms": sweep_ms},
+        "gpu_launches": tm["kernel_launches"],
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_reference_sample(d, args.cpu_inners)
+        if cb is not None:
+            line["cpu_baseline"] = cb
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+    snap.close()
+    return 0
+
+
+def main():
+    global GROUPS
+    args = parse()
+    GROUPS = args.groups
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_snap(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -118,6 +118,28 @@ int snap_sweep(snap_ctx *ctx, const void *qtot, const void *t_xs, void *flux, vo
 int snap_test_convergence(snap_ctx *ctx, int kind, const double *flux, const double *prev,
                           double epsi, int *converged, void *stream);
 
+/* One inner iteration on device-resident data, the body of the reference's
+ * inner loop (snap.cc:487-503: CalcInnerSource, save_fluxes, MiniKBATask for
+ * every octant and group, TestInnerConvergence):
+ *   qtot  = q2grp + flux * s_xs            (scratch supplied by the caller,
+ *                                           sweep precision, G*C*cmom words)
+ *   flux  = sweep(qtot, t_xs)              (in place, double, cmom moments)
+ *   *converged = inner test of the new scalar flux against the old one.
+ * t_xs has the sweep precision.  *converged is HOST memory; the call
+ * synchronises `stream`. */
+int snap_inner_iteration(snap_ctx *ctx, const double *s_xs, const double *q2grp,
+                         const void *t_xs, double *flux, void *qtot, double epsi,
+                         int *converged, void *stream);
+
+typedef struct {
+  double sweep_ms;          /* device time of the sweep kernels (CUDA events) */
+  long long sweep_calls;    /* sweeps timed */
+  long long kernel_launches;/* kernels this library launched */
+} snap_timing;
+
+/* Accumulated timing of this context since creation or the last reset. */
+int snap_get_timing(snap_ctx *ctx, snap_timing *out, int reset);
+
 typedef struct {
   double epsi;
   int iitm, oitm;

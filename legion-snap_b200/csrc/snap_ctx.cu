@@ -58,7 +58,10 @@ struct snap_ctx {
   int *d_ctrl = nullptr;   // [n_items progress][counter][error][violations]
   int *h_ctrl = nullptr;   // pinned: error, violations
   size_t scratch_bytes = 0;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;   // whole-solve timing
+  cudaEvent_t sw0 = nullptr, sw1 = nullptr;   // sweep timing
+  double sweep_ms = 0.0;
+  long long sweep_calls = 0, launches = 0;
 
   int *progress() { return d_ctrl; }
   int *counter() { return d_ctrl + n_items; }
@@ -82,6 +85,8 @@ void free_ctx(snap_ctx *c) {
   if (c->h_ctrl) cudaFreeHost(c->h_ctrl);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->sw0) cudaEventDestroy(c->sw0);
+  if (c->sw1) cudaEventDestroy(c->sw1);
   delete c;
 }
 
@@ -178,8 +183,31 @@ int sweep_launches(snap_ctx *c, const void *qtot, const void *t_xs, cudaStream_t
     cudaError_t e = c->fp32 ? launch_sweep_fp32(c->shape, p, c->grid, st)
                             : launch_sweep_fp64(c->shape, p, c->grid, st);
     if (e != cudaSuccess) return cuda_fail(e, "sweep launch");
+    ++c->launches;
   }
   return SNAP_OK;
+}
+
+// Sweep plus the octant-slot reduction into `flux` (with the inner test when
+// test != 0), bracketed by the context's sweep events.
+int timed_sweep(snap_ctx *c, const void *qtot, const void *t_xs, void *flux, int flux_fp32,
+                double *flux64, int test, double epsi, cudaStream_t st) {
+  SNAP_CUDA(cudaEventRecord(c->sw0, st));
+  int rc = sweep_launches(c, qtot, t_xs, st);
+  if (rc) return rc;
+  SNAP_CUDA(cudaEventRecord(c->sw1, st));
+  SNAP_CUDA(k_reduce_slots(c->d_slots, c->P, c->fp32, flux, flux_fp32, flux64, c->cfg.ng, c->M,
+                           c->C, test, epsi, c->violations(), st));
+  ++c->launches;
+  return SNAP_OK;
+}
+
+void account_sweep(snap_ctx *c) {
+  float ms = 0.0f;
+  if (cudaEventElapsedTime(&ms, c->sw0, c->sw1) == cudaSuccess) {
+    c->sweep_ms += ms;
+    ++c->sweep_calls;
+  }
 }
 
 // Reads the device error word and the violation counter (synchronises).
@@ -307,7 +335,8 @@ int snap_create(const snap_config *cfg, int device, snap_ctx **out) {
   c->scratch_bytes = slots_b + bx_b + by_b + sizeof(int) * (c->n_items + 3);
   if (cudaMemset(c->d_ctrl, 0, sizeof(int) * (c->n_items + 3)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_ctrl, 4 * sizeof(int)) != cudaSuccess ||
-      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+      cudaEventCreate(&c->sw0) != cudaSuccess || cudaEventCreate(&c->sw1) != cudaSuccess) {
     free_ctx(c);
     return fail(SNAP_ERR_CUDA, "context setup failed");
   }
@@ -336,6 +365,7 @@ size_t snap_scratch_bytes(const snap_ctx *ctx) { return ctx ? ctx->scratch_bytes
 int snap_expand_xs(snap_ctx *c, const double *sig, const int32_t *mat, double *xs, void *stream) {
   if (!c || !sig || !mat || !xs) return fail(SNAP_ERR_BAD_ARG, "null argument");
   SNAP_CUDA(k_expand_xs(sig, mat, xs, c->cfg.ng, c->cfg.nmat, c->C, (cudaStream_t)stream));
+  ++c->launches;
   return SNAP_OK;
 }
 
@@ -344,6 +374,7 @@ int snap_expand_scattering_xs(snap_ctx *c, const double *slgg, const int32_t *ma
   if (!c || !slgg || !mat || !s_xs) return fail(SNAP_ERR_BAD_ARG, "null argument");
   SNAP_CUDA(k_expand_scat(slgg, mat, s_xs, c->cfg.ng, c->cfg.nmat, c->cfg.nmom, c->C,
                           (cudaStream_t)stream));
+  ++c->launches;
   return SNAP_OK;
 }
 
@@ -352,6 +383,7 @@ int snap_calc_outer_source(snap_ctx *c, const double *qi, const double *slgg, co
   if (!c || !qi || !slgg || !mat || !flux || !q2grp) return fail(SNAP_ERR_BAD_ARG, "null argument");
   SNAP_CUDA(k_outer_source(qi, slgg, mat, flux, q2grp, c->cfg.ng, c->cfg.nmat, c->cfg.nmom, c->M,
                            c->C, (cudaStream_t)stream));
+  ++c->launches;
   return SNAP_OK;
 }
 
@@ -360,6 +392,7 @@ int snap_calc_inner_source(snap_ctx *c, const double *s_xs, const double *q2grp,
   if (!c || !s_xs || !q2grp || !flux || !qtot) return fail(SNAP_ERR_BAD_ARG, "null argument");
   SNAP_CUDA(k_inner_source(s_xs, q2grp, flux, qtot, c->fp32, c->cfg.ng, c->cfg.nmom, c->M, c->C,
                            (cudaStream_t)stream));
+  ++c->launches;
   return SNAP_OK;
 }
 
@@ -367,11 +400,43 @@ int snap_sweep(snap_ctx *c, const void *qtot, const void *t_xs, void *flux, void
   if (!c || !qtot || !t_xs || !flux) return fail(SNAP_ERR_BAD_ARG, "null argument");
   cudaStream_t st = (cudaStream_t)stream;
   SNAP_CUDA(cudaMemsetAsync(c->error(), 0, 2 * sizeof(int), st));
-  int rc = sweep_launches(c, qtot, t_xs, st);
+  int rc = timed_sweep(c, qtot, t_xs, flux, c->fp32, nullptr, 0, 0.0, st);
   if (rc) return rc;
-  SNAP_CUDA(k_reduce_slots(c->d_slots, c->P, c->fp32, flux, c->fp32, nullptr, c->cfg.ng, c->M,
-                           c->C, 0, 0.0, nullptr, st));
-  return read_ctrl(c, st, nullptr);
+  rc = read_ctrl(c, st, nullptr);
+  if (rc == SNAP_OK) account_sweep(c);
+  return rc;
+}
+
+int snap_inner_iteration(snap_ctx *c, const double *s_xs, const double *q2grp, const void *t_xs,
+                         double *flux, void *qtot, double epsi, int *converged, void *stream) {
+  if (!c || !s_xs || !q2grp || !t_xs || !flux || !qtot || !converged)
+    return fail(SNAP_ERR_BAD_ARG, "null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  SNAP_CUDA(cudaMemsetAsync(c->error(), 0, 2 * sizeof(int), st));
+  SNAP_CUDA(k_inner_source(s_xs, q2grp, flux, qtot, c->fp32, c->cfg.ng, c->cfg.nmom, c->M, c->C,
+                           st));
+  ++c->launches;
+  int rc = timed_sweep(c, qtot, t_xs, flux, 0, flux, 1, epsi, st);
+  if (rc) return rc;
+  int v = 0;
+  rc = read_ctrl(c, st, &v);
+  if (rc) return rc;
+  account_sweep(c);
+  *converged = v == 0;
+  return SNAP_OK;
+}
+
+int snap_get_timing(snap_ctx *c, snap_timing *out, int reset) {
+  if (!c || !out) return fail(SNAP_ERR_BAD_ARG, "null argument");
+  out->sweep_ms = c->sweep_ms;
+  out->sweep_calls = c->sweep_calls;
+  out->kernel_launches = c->launches;
+  if (reset) {
+    c->sweep_ms = 0.0;
+    c->sweep_calls = 0;
+    c->launches = 0;
+  }
+  return SNAP_OK;
 }
 
 int snap_test_convergence(snap_ctx *c, int kind, const double *flux, const double *prev,
@@ -382,6 +447,7 @@ int snap_test_convergence(snap_ctx *c, int kind, const double *flux, const doubl
   SNAP_CUDA(cudaMemsetAsync(c->error(), 0, 2 * sizeof(int), st));
   SNAP_CUDA(k_count_violations(flux, prev, c->M, (long long)c->cfg.ng * c->C, epsi,
                                c->violations(), st));
+  ++c->launches;
   int v = 0;
   int rc = read_ctrl(c, st, &v);
   if (rc) return rc;
@@ -431,6 +497,7 @@ int snap_transport_solve(snap_ctx *c, const int32_t *mat, const double *qi, cons
   {
     info->inner_total = info->outer_total = info->converged = 0;
     info->sweep_ms = info->total_ms = 0.0;
+    const double sweep_ms0 = c->sweep_ms;
     float ms = 0.0f;
     STEP(cudaMemsetAsync(c->error(), 0, 2 * sizeof(int), st));
     STEP(cudaEventRecord(c->ev0, st));
@@ -438,6 +505,7 @@ int snap_transport_solve(snap_ctx *c, const int32_t *mat, const double *qi, cons
     STEP(k_expand_xs(sigt, mat, t_xs64, G, c->cfg.nmat, C, st));
     if (sigt_scale) STEP(k_scale_xs(t_xs64, sigt_scale, G, C, st));
     STEP(k_expand_scat(slgg, mat, s_xs, G, c->cfg.nmat, nmom, C, st));
+    c->launches += sigt_scale ? 3 : 2;
     if (c->fp32) {
       if (cudaMalloc(&t_xs_sw, sizeof(float) * n) != cudaSuccess) {
         t_xs_sw = t_xs64;
@@ -445,27 +513,22 @@ int snap_transport_solve(snap_ctx *c, const int32_t *mat, const double *qi, cons
         goto done;
       }
       STEP(k_to_f32(t_xs64, (float *)t_xs_sw, n, st));
+      ++c->launches;
     }
     STEP(cudaMemsetAsync(flux, 0, sizeof(double) * n * M, st));   // snap.cc:313-316
     for (int o = 0; o < info->oitm; ++o) {
       STEP(k_outer_source(qi, slgg, mat, flux, q2grp, G, c->cfg.nmat, nmom, M, C, st));
       STEP(k_copy_moment0(flux, fpo, M, n, st));                   // save_fluxes -> flux0po
+      c->launches += 2;
       bool inner_conv = false;
       int inners = 0;
       for (int i = 0; i < info->iitm; ++i) {
-        STEP(k_inner_source(s_xs, q2grp, flux, qtot, c->fp32, G, nmom, M, C, st));
-        STEP(cudaMemsetAsync(c->violations(), 0, sizeof(int), st));
-        rc = sweep_launches(c, qtot, t_xs_sw, st);
-        if (rc) goto done;
-        // flux = sum of octant slots, inner test against the previous flux
-        STEP(k_reduce_slots(c->d_slots, c->P, c->fp32, flux, 0, flux, G, M, C, 1, info->epsi,
-                            c->violations(), st));
-        int v = 0;
-        rc = read_ctrl(c, st, &v);
+        int conv = 0;
+        rc = snap_inner_iteration(c, s_xs, q2grp, t_xs_sw, flux, qtot, info->epsi, &conv, st);
         if (rc) goto done;
         ++inners;
         ++info->inner_total;
-        inner_conv = v == 0;
+        inner_conv = conv != 0;
         if (inner_conv) break;
       }
       if (o < 1024) info->inners_per_outer[o] = inners;
@@ -474,6 +537,7 @@ int snap_transport_solve(snap_ctx *c, const int32_t *mat, const double *qi, cons
       if (inner_conv) {
         STEP(cudaMemsetAsync(c->violations(), 0, sizeof(int), st));
         STEP(k_count_violations(flux, fpo, M, n, 100.0 * info->epsi, c->violations(), st));
+        ++c->launches;
         int v = 0;
         rc = read_ctrl(c, st, &v);
         if (rc) goto done;
@@ -487,6 +551,7 @@ int snap_transport_solve(snap_ctx *c, const int32_t *mat, const double *qi, cons
     STEP(cudaEventSynchronize(c->ev1));
     STEP(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
     info->total_ms = ms;
+    info->sweep_ms = c->sweep_ms - sweep_ms0;
   }
 done:
   cleanup();

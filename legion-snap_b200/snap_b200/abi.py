@@ -33,6 +33,11 @@ class SnapSolveInfo(C.Structure):
                 ("total_ms", C.c_double)]
 
 
+class SnapTiming(C.Structure):
+    _fields_ = [("sweep_ms", C.c_double), ("sweep_calls", C.c_longlong),
+                ("kernel_launches", C.c_longlong)]
+
+
 class SnapError(RuntimeError):
     def __init__(self, status: int, msg: str):
         super().__init__(f"{STATUS.get(status, status)}: {msg}")
@@ -51,6 +56,8 @@ SIGNATURES = {
     "snap_calc_inner_source": [_vp, _vp, _vp, _vp, _vp, _vp],
     "snap_sweep": [_vp, _vp, _vp, _vp, _vp],
     "snap_test_convergence": [_vp, C.c_int, _vp, _vp, C.c_double, _ip, _vp],
+    "snap_inner_iteration": [_vp, _vp, _vp, _vp, _vp, _vp, C.c_double, _ip, _vp],
+    "snap_get_timing": [_vp, C.POINTER(SnapTiming), C.c_int],
     "snap_transport_solve": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, C.POINTER(SnapSolveInfo), _vp],
     "snap_last_error": [],
 }

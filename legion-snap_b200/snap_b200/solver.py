@@ -129,6 +129,21 @@ class Snap:
             return False
         return self._test(1, flux, flux_po, 100.0 * self.deck.epsi)
 
+    def inner_iteration(self, s_xs, q2grp, t_xs, flux, qtot, epsi=None) -> bool:
+        """One inner iteration on resident data (snap.cc:487-503); flux is
+        updated in place, qtot is scratch.  Returns the inner test result."""
+        conv = C.c_int(0)
+        abi.check(self.lib.snap_inner_iteration(
+            self.handle, _ptr(s_xs), _ptr(q2grp), _ptr(t_xs), _ptr(flux), _ptr(qtot),
+            C.c_double(self.deck.epsi if epsi is None else epsi), C.byref(conv), _stream()))
+        return bool(conv.value)
+
+    def timing(self, reset: bool = False) -> dict:
+        t = abi.SnapTiming()
+        abi.check(self.lib.snap_get_timing(self.handle, C.byref(t), int(reset)))
+        return dict(sweep_ms=t.sweep_ms, sweep_calls=t.sweep_calls,
+                    kernel_launches=t.kernel_launches)
+
     # ---- the solve loop ----------------------------------------------------
     def device_problem(self, prob: dict) -> dict:
         dev = self.device
@@ -161,5 +176,5 @@ class Snap:
         rec = dict(inner_total=info.inner_total, outer_total=info.outer_total,
                    converged=bool(info.converged),
                    inners_per_outer=list(info.inners_per_outer[:info.outer_total]),
-                   total_ms=info.total_ms)
+                   total_ms=info.total_ms, sweep_ms=info.sweep_ms)
         return flux, rec
