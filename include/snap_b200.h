@@ -159,6 +159,29 @@ int snap_transport_solve(snap_ctx *ctx, const int32_t *mat, const double *qi,
                          const double *sigt, const double *slgg, const double *sigt_scale,
                          double *flux, snap_solve_info *info, void *stream);
 
+/* Size of the static device scratch that snap_sweep_noalloc works in. */
+#define SNAP_NOALLOC_SCRATCH_BYTES (48u << 20)
+
+/* The FP64 sweep of snap_sweep (all octants and groups; flux zeroed first)
+ * for callers that cannot allocate device memory: code running where
+ * cudaMalloc is unavailable or forbidden (inside another library's
+ * allocator-free section, a host callback, a process whose device memory
+ * pool belongs to someone else, a real-time loop that must not touch the
+ * allocator), which therefore cannot call snap_create.
+ * Takes the configuration directly (cfg->precision must be SNAP_FP64; host
+ * quadrature arrays as for snap_create) and device qtot, t_xs and flux
+ * arrays as snap_sweep does.  It allocates nothing: its scratch is one
+ * static device array of SNAP_NOALLOC_SCRATCH_BYTES bytes that every GPU
+ * loading this library holds until exit, and problems needing more return
+ * SNAP_ERR_UNSUPPORTED with the size in snap_last_error().  Every call
+ * shares that array (it keeps the last call's contents; each call clears
+ * what must start at zero), so calls that overlap on the GPU race.  The
+ * first call on a device looks the array's device address up; make it before
+ * any stream capture on that device.  Synchronises `stream`.
+ * No counterpart in the reference. */
+int snap_sweep_noalloc(const snap_config *cfg, const double *qtot, const double *t_xs,
+                       double *flux, void *stream);
+
 /* Last error message of this thread (static storage). */
 const char *snap_last_error(void);
 

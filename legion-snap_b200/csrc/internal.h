@@ -46,6 +46,9 @@ struct SweepShape {
   int TY;   // warps per CTA = tile rows in y
 };
 
+// Records the message snap_last_error() returns; returns `code`.
+int set_last_error(int code, const std::string &msg);
+
 // Error codes written to the device error word.
 enum : int { DEV_ERR_NONE = 0, DEV_ERR_TIMEOUT = 1 };
 

@@ -37,6 +37,8 @@ int cuda_fail(cudaError_t e, const char *what) {
 
 }  // namespace
 
+int snapb200::set_last_error(int code, const std::string &msg) { return fail(code, msg); }
+
 struct snap_ctx {
   snap_config cfg{};
   std::vector<double> mu, eta, xi, w, ec;
