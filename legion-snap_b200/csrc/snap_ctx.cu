@@ -237,8 +237,10 @@ int snap_create(const snap_config *cfg, int device, snap_ctx **out) {
     return fail(SNAP_ERR_BAD_ARG, "invalid configuration");
   if (cfg->precision != SNAP_FP64 && cfg->precision != SNAP_FP32)
     return fail(SNAP_ERR_BAD_ARG, "unknown precision");
-  if (cfg->nx % 8 || cfg->ny % 8)
-    return fail(SNAP_ERR_UNSUPPORTED, "nx and ny must be multiples of 8");
+  int tile_y = cfg->ny % 4 == 0 ? 4 : 8;
+  if (const char *te = getenv("SNAP_B200_TILE_Y")) tile_y = atoi(te) == 8 ? 8 : 4;
+  if (cfg->nx % 8 || cfg->ny % tile_y)
+    return fail(SNAP_ERR_UNSUPPORTED, "nx must be a multiple of 8 and ny of the tile height");
   if (cfg->nang > 64) return fail(SNAP_ERR_UNSUPPORTED, "at most 64 angles per octant");
   if (cfg->nx / 8 > 255 || cfg->ny / 8 > 255)
     return fail(SNAP_ERR_UNSUPPORTED, "at most 2040 cells along x and y");
@@ -266,7 +268,7 @@ int snap_create(const snap_config *cfg, int device, snap_ctx **out) {
   c->shape.NT = (c->A + 7) / 8;
   c->shape.MK = c->M == 1 ? 0 : (c->M + 3) / 4;
   c->shape.MN = c->shape.MK == 0 ? 0 : (c->shape.MK + 1) / 2;
-  c->shape.TY = 8;
+  c->shape.TY = tile_y;
   c->AP = 8 * c->shape.NT;
   c->wsize = c->fp32 ? sizeof(float) : sizeof(double);
   const bool ok = c->fp32 ? sweep_fp32_supported(c->shape) : sweep_fp64_supported(c->shape);
