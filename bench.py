@@ -58,6 +58,7 @@ def parse():
     ap.add_argument("--e2e-solves", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-inners", type=int, default=2)
+    ap.add_argument("--no-mixed", action="store_true", help="skip the FP32 leg")
     ap.add_argument("--groups", type=int, default=None,
                     help="override deck 2's 32 groups (small cases for profiling only)")
     return ap.parse_args()
@@ -314,6 +315,46 @@ def run_snap(args):
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
     e2e = float(e2e_t.item()) / world
 
+    # mixed-precision form on the same deck: FP32 sweep (FP64 octant sums,
+    # sources and convergence); grind time and scalar-flux error against the
+    # FP64 solve above
+    mixed = None
+    if not args.no_mixed:
+        snap32 = Snap(d, precision="fp32", device=local)
+        t_xs32 = t_xs.float()
+        flux32 = torch.zeros(d.ng, d.cells, d.cmom, dtype=torch.float64, device="cuda")
+        q2grp32 = snap32.calc_outer_source(dp["qi"], dp["slgg"], dp["mat"], flux32)
+        qtot32 = torch.empty(d.ng, d.cells, d.cmom, dtype=torch.float32, device="cuda")
+        for _ in range(args.warmup):
+            snap32.inner_iteration(s_xs, q2grp32, t_xs32, flux32, qtot32)
+        torch.cuda.synchronize()
+        snap32.timing(reset=True)
+        ev0.record()
+        for _ in range(args.steps):
+            snap32.inner_iteration(s_xs, q2grp32, t_xs32, flux32, qtot32)
+        ev1.record()
+        torch.cuda.synchronize()
+        ms32 = ev0.elapsed_time(ev1) / args.steps
+        tm32 = snap32.timing()
+        sweep32 = tm32["sweep_ms"] / max(tm32["sweep_calls"], 1)
+        mixed = {"precision": "fp32 sweep (moment contractions on FP64 tensor cores), "
+                              "fp64 octant sums, sources, convergence",
+                 "value": ms32 * 1e6 / d.units_per_sweep, "unit": UNIT, "ms_per_step": ms32,
+                 "speedup_vs_fp64": ms_per_step / ms32, "sweep_ms": sweep32,
+                 "roofline": {"bound": "hbm", "bytes_per_unit": (3 * d.cmom + 1) * 4 / d.nang,
+                              "achieved": (3 * d.cmom + 1) * 4 / d.nang * d.units_per_sweep
+                                          / (sweep32 * 1e-3) / 1e9, "peak": peak}}
+        mixed["roofline"]["frac"] = mixed["roofline"]["achieved"] / peak
+        if e2e_vals:   # whole mixed solve against the FP64 solve of the e2e leg
+            f32, rec32 = snap32.transport_solve(dp)
+            ref = out[..., 0]
+            diff = (f32[..., 0] - ref).abs() / ref.abs().clamp_min(1e-300)
+            mixed["max_rel_err_scalar_flux"] = float(diff.max())
+            mixed["rms_rel_err_scalar_flux"] = float(diff.pow(2).mean().sqrt())
+            mixed["inner_iterations"] = rec32["inner_total"]
+            mixed["fp64_inner_iterations"] = rec["inner_total"]
+        snap32.close()
+
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
@@ -330,6 +371,8 @@ def run_snap(args):
         "gpu_launches": tm["kernel_launches"],
         "clocks": clk,
     }
+    if mixed is not None:
+        line["mixed_precision"] = mixed
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_reference_sample(d, args.cpu_inners)
         if cb is not None:

@@ -99,10 +99,12 @@ int upload(void **dst, const std::vector<T> &v) {
   return SNAP_OK;
 }
 
-// Per-octant MMA operand tables in the lane order of the m8n8k4 fragments.
+// Per-octant MMA operand tables in the lane order of the m8n8k4 fragments
+// (always double: both precisions contract on the FP64 tensor cores) and the
+// per-angle coefficients in the sweep precision T.
 template <typename T>
-void build_tables(const snap_ctx *c, std::vector<T> &coef, std::vector<T> &bt1,
-                  std::vector<T> &bt2) {
+void build_tables(const snap_ctx *c, std::vector<T> &coef, std::vector<double> &bt1,
+                  std::vector<double> &bt2) {
   const int AP = c->AP, NT = c->shape.NT, MK = c->shape.MK, MN = c->shape.MN, M = c->M,
             A = c->A;
   coef.assign(4 * AP, T(0));
@@ -114,14 +116,14 @@ void build_tables(const snap_ctx *c, std::vector<T> &coef, std::vector<T> &bt1,
   }
   auto ec = [&](int o, int m, int a) { return c->ec[((size_t)o * M + m) * A + a]; };
   const int B1 = MK * NT * 32, B2 = 2 * NT * MN * 32;
-  bt1.assign((size_t)8 * B1, T(0));
-  bt2.assign((size_t)8 * B2, T(0));
+  bt1.assign((size_t)8 * B1, 0.0);
+  bt2.assign((size_t)8 * B2, 0.0);
   for (int o = 0; o < 8; ++o) {
     for (int kt = 0; kt < MK; ++kt)
       for (int nt = 0; nt < NT; ++nt)
         for (int l = 0; l < 32; ++l) {
           const int m = (l & 3) * MK + kt, a = 8 * nt + (l >> 2);
-          bt1[(size_t)o * B1 + (kt * NT + nt) * 32 + l] = (m < M && a < A) ? (T)ec(o, m, a) : T(0);
+          bt1[(size_t)o * B1 + (kt * NT + nt) * 32 + l] = (m < M && a < A) ? ec(o, m, a) : 0.0;
         }
     for (int t = 0; t < 2 * NT; ++t)
       for (int mt = 0; mt < MN; ++mt)
@@ -131,7 +133,7 @@ void build_tables(const snap_ctx *c, std::vector<T> &coef, std::vector<T> &bt1,
           const int r = l >> 2;
           const int m = (r >> 1) * 2 * MN + 2 * mt + (r & 1);
           bt2[(size_t)o * B2 + (t * MN + mt) * 32 + l] =
-              (m < M && a < A) ? (T)(ec(o, m, a) * c->w[a]) : T(0);
+              (m < M && a < A) ? ec(o, m, a) * c->w[a] : 0.0;
         }
   }
 }
@@ -287,7 +289,8 @@ int snap_create(const snap_config *cfg, int device, snap_ctx **out) {
   }
   // tables
   if (c->fp32) {
-    std::vector<float> coef, bt1, bt2;
+    std::vector<float> coef;
+    std::vector<double> bt1, bt2;
     build_tables<float>(c, coef, bt1, bt2);
     if ((rc = upload(&c->d_coef, coef)) || (rc = upload(&c->d_bt1, bt1)) ||
         (rc = upload(&c->d_bt2, bt2))) {

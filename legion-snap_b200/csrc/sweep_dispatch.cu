@@ -1,0 +1,63 @@
+// Entry points of the sweep kernels: shape dispatch over the per-precision,
+// per-angle-tile translation units (the kernel itself is in sweep.cuh).
+#include "sweep.cuh"
+
+namespace snapb200 {
+namespace {
+
+using DispatchFn = cudaError_t (*)(int, int, int, const SweepParams *, int, cudaStream_t, int *,
+                                   size_t *);
+const DispatchFn kFp64[9] = {nullptr,
+                             sweep_fp64_dispatch_nt1, sweep_fp64_dispatch_nt2,
+                             sweep_fp64_dispatch_nt3, sweep_fp64_dispatch_nt4,
+                             sweep_fp64_dispatch_nt5, sweep_fp64_dispatch_nt6,
+                             sweep_fp64_dispatch_nt7, sweep_fp64_dispatch_nt8};
+const DispatchFn kFp32[9] = {nullptr,
+                             sweep_fp32_dispatch_nt1, sweep_fp32_dispatch_nt2,
+                             sweep_fp32_dispatch_nt3, sweep_fp32_dispatch_nt4,
+                             sweep_fp32_dispatch_nt5, sweep_fp32_dispatch_nt6,
+                             sweep_fp32_dispatch_nt7, sweep_fp32_dispatch_nt8};
+
+bool supported(const SweepShape &sh) {
+  return (sh.TY == 8 || sh.TY == 4) && sh.NT >= 1 && sh.NT <= 8 && sh.MK >= 0 && sh.MK <= 4;
+}
+
+cudaError_t dispatch(const DispatchFn *table, const SweepShape &sh, int op, const SweepParams *p,
+                     int grid, cudaStream_t st, int *blocks, size_t *smem) {
+  if (!supported(sh)) return cudaErrorInvalidValue;
+  return table[sh.NT](sh.MK, sh.TY, op, p, grid, st, blocks, smem);
+}
+
+}  // namespace
+
+bool sweep_fp64_supported(const SweepShape &sh) { return supported(sh); }
+bool sweep_fp32_supported(const SweepShape &sh) { return supported(sh); }
+
+cudaError_t launch_sweep_fp64(const SweepShape &sh, const SweepParams &p, int grid,
+                              cudaStream_t st) {
+  return dispatch(kFp64, sh, 0, &p, grid, st, nullptr, nullptr);
+}
+cudaError_t launch_sweep_fp32(const SweepShape &sh, const SweepParams &p, int grid,
+                              cudaStream_t st) {
+  return dispatch(kFp32, sh, 0, &p, grid, st, nullptr, nullptr);
+}
+
+cudaError_t sweep_fp64_occupancy(const SweepShape &sh, int *blocks_per_sm, size_t *smem) {
+  return dispatch(kFp64, sh, 1, nullptr, 0, nullptr, blocks_per_sm, smem);
+}
+cudaError_t sweep_fp32_occupancy(const SweepShape &sh, int *blocks_per_sm, size_t *smem) {
+  return dispatch(kFp32, sh, 1, nullptr, 0, nullptr, blocks_per_sm, smem);
+}
+
+size_t sweep_fp64_smem(const SweepShape &sh) {
+  size_t smem = 0;
+  dispatch(kFp64, sh, 2, nullptr, 0, nullptr, nullptr, &smem);
+  return smem;
+}
+size_t sweep_fp32_smem(const SweepShape &sh) {
+  size_t smem = 0;
+  dispatch(kFp32, sh, 2, nullptr, 0, nullptr, nullptr, &smem);
+  return smem;
+}
+
+}  // namespace snapb200

@@ -1,0 +1,10 @@
+// Instantiates the fp32 sweep shapes with 5 angle tile(s) of 8 (one file per
+// precision and angle-tile count, so the shapes compile in parallel).
+#include "sweep.cuh"
+
+namespace snapb200 {
+cudaError_t sweep_fp32_dispatch_nt5(int mk, int ty, int op, const SweepParams *p, int grid,
+                                    cudaStream_t st, int *blocks, size_t *smem) {
+  return sw::dispatch_nt<float, 5>(mk, ty, op, p, grid, st, blocks, smem);
+}
+}  // namespace snapb200

@@ -234,3 +234,53 @@ def test_solve_deck2_full_size_properties():
     assert (phi > 0).all()
     for dim in (1, 2, 3):
         assert rel_err(phi.flip(dim).cpu().numpy(), phi.cpu().numpy()) < TOL
+
+
+# ---------------------------------------------------------------- FP32 form
+FP32_TOL = 1e-5    # scalar-flux error of the FP32 form against the FP64 oracle
+
+
+def snap_ctx32(deck):
+    from snap_b200.solver import Snap
+    return Snap(deck, precision="fp32")
+
+
+@pytest.mark.parametrize("d", [P.deck(1), P.Deck(16, 16, 16, nang=36, ng=3, nmom=4)],
+                         ids=["deck1", "A36_cmom16"])
+def test_fp32_sweep_error(d):
+    prob = P.make_problem(d)
+    o = Oracle(d)
+    t_xs, _ = o.expand(prob)
+    qtot = random_qtot(d, 11)
+    ref = o.sweep(qtot, t_xs)
+    snap = snap_ctx32(d)
+    got = snap.mini_kba_sweep(dev(qtot).float(), dev(t_xs).float()).double().cpu().numpy()
+    assert rel_err(got[..., 0], ref[..., 0]) < FP32_TOL
+    assert moment_err(got, ref) < FP32_TOL
+
+
+def test_fp32_sweep_fixup_heavy():
+    d = P.Deck(16, 16, 8, nang=10, ng=2, nmom=2)
+    prob = thick_point_source(d)
+    o = Oracle(d)
+    t_xs, s_xs = o.expand(prob)
+    q2 = o.outer_source(prob, np.zeros((d.ng, d.cells, d.cmom)))
+    qtot = o.inner_source(s_xs, q2, np.zeros((d.ng, d.cells, d.cmom)))
+    ref = o.sweep(qtot, t_xs)
+    got = snap_ctx32(d).mini_kba_sweep(dev(qtot).float(), dev(t_xs).float()).double().cpu().numpy()
+    # thick cells: values span many decades; compare where the flux is not tiny
+    phi, rphi = got[..., 0], ref[..., 0]
+    big = np.abs(rphi) > 1e-6 * np.abs(rphi).max()
+    assert rel_err(phi[big], rphi[big]) < 1e-4
+
+
+@pytest.mark.parametrize("d", [P.deck(1), P.Deck(16, 16, 16, nang=12, ng=4, nmom=4, epsi=1e-6,
+                                                 iitm=3, oitm=4)], ids=["deck1", "cmom16"])
+def test_fp32_solve_error(d):
+    """The mixed-precision solve (FP32 sweep, FP64 sources, octant sums and
+    convergence) stays within 1e-5 of the FP64 oracle in scalar flux."""
+    prob = P.make_problem(d)
+    ref, _ = Oracle(d).solve(prob)
+    snap = snap_ctx32(d)
+    flux, rec = snap.transport_solve(snap.device_problem(prob))
+    assert rel_err(flux[..., 0].cpu().numpy(), ref[..., 0]) < FP32_TOL
