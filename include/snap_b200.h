@@ -159,6 +159,42 @@ int snap_transport_solve(snap_ctx *ctx, const int32_t *mat, const double *qi,
                          const double *sigt, const double *slgg, const double *sigt_scale,
                          double *flux, snap_solve_info *info, void *stream);
 
+/* ---- Sensitivities (no counterpart in the reference) ------------------ */
+
+/* A forward sweep (as snap_sweep) that also records, for the adjoint, the
+ * cell-average angular flux and the fixup face flags of every octant, angle,
+ * group and cell in the context (8*G*C*padded-angles words + bytes). */
+int snap_record_forward(snap_ctx *ctx, const void *qtot, const void *t_xs, void *flux,
+                        void *stream);
+
+/* One adjoint sweep of all octants and groups: the transpose of the sweep
+ * operator (reverse-direction wavefront, transposed diamond difference with
+ * the recorded fixup flags frozen) applied to the adjoint flux moments
+ * phi_bar [G][C][cmom] (sweep precision): qtot_bar [G][C][cmom] (double) =
+ * M^T L^-T D^T phi_bar.  With sigt_bar != NULL also the sensitivity to the
+ * expanded total cross section, sigt_bar [G][C] = -sum_{octant,angle} s*pc,
+ * from the recorded forward state.  Needs snap_record_forward first when the
+ * fixup is on or sigt_bar is wanted.  Synchronises `stream`. */
+int snap_adjoint_sweep(snap_ctx *ctx, const void *phi_bar, const void *t_xs, double *qtot_bar,
+                       double *sigt_bar, void *stream);
+
+/* Discrete adjoint of the converged steady-state solve.  Given the expanded
+ * total cross section t_xs [G][C] (double) the forward solve used, the
+ * converged forward flux (double, cmom moments) and a response J = sum
+ * r[g][c] * flux[g][c][0], iterates phi_bar = r + S^T M^T L^-T D^T phi_bar
+ * (S: the full group-to-group scattering, in-group included; fixup flags
+ * frozen at the forward state) until max|change| <= info->epsi *
+ * max|phi_bar| (at most iitm*oitm iterations; info->inner_total reports
+ * them) and returns dJ/dt_xs [G][C] (per-cell, per-group total cross
+ * section), dJ/dqi [G][C] (fixed source) and, when grad_sxs != NULL,
+ * dJ/ds_xs [G][C][nmom] (per-cell in-group scattering).  Angular fluxes are
+ * never stored across iterations: the forward state is recomputed once from
+ * the flux moments. */
+int snap_adjoint_solve(snap_ctx *ctx, const int32_t *mat, const double *qi, const double *t_xs,
+                       const double *slgg, const double *flux, const double *response,
+                       double *grad_sigt, double *grad_qi, double *grad_sxs,
+                       snap_solve_info *info, void *stream);
+
 /* Size of the static device scratch that snap_sweep_noalloc works in. */
 #define SNAP_NOALLOC_SCRATCH_BYTES (48u << 20)
 

@@ -36,6 +36,14 @@ struct SweepParams {
   const void *bt1;        // [8][MK][NT][32] source-expansion fragments
   const void *bt2;        // [8][2NT][MN][32] moment-accumulation fragments
   const void *coef;       // [4][AP]: hi*mu, hj*eta, hk*xi, w
+  // Optional forward-state store for the adjoint (null when not wanted):
+  // cell-average angular flux and fixup flags of every (octant, group, cell,
+  // padded angle): bits 0-2 = outgoing face x, y, z kept, bit 3 = flux forced
+  // to 0, bits 4-6 = faces kept in the last recompute of the flux.
+  void *pc_store;         // [8][G][C][AP]
+  uint8_t *flag_store;    // [8][G][C][AP]
+  // Adjoint sweep only: the adjoint of t_xs per octant slot, [P][G][C].
+  void *sigt_bar_slots;
 };
 
 // Per-precision static configuration picked at context creation.
@@ -65,6 +73,11 @@ cudaError_t sweep_fp32_occupancy(const SweepShape &sh, int *blocks_per_sm, size_
 size_t sweep_fp32_smem(const SweepShape &sh);
 bool sweep_fp32_supported(const SweepShape &sh);
 
+// adjoint sweep kernels (adjoint_dispatch.cu); op 0 launch, 1 occupancy, 2 smem
+bool adjoint_supported(const SweepShape &sh);
+cudaError_t adjoint_dispatch(int fp32, const SweepShape &sh, int op, const SweepParams *p, int grid,
+                             cudaStream_t st, int *blocks, size_t *smem);
+
 // small kernels (kernels.cu)
 cudaError_t k_expand_xs(const double *sig, const int32_t *mat, double *xs, int G, int nmat,
                         long long C, cudaStream_t st);
@@ -85,6 +98,19 @@ cudaError_t k_reduce_slots(const void *slots, int nslots, int fp32, void *flux_o
 cudaError_t k_count_violations(const double *flux, const double *prev, int M, long long n,
                                double epsi, int *violations, cudaStream_t st);
 cudaError_t k_to_f32(const double *in, float *out, long long n, cudaStream_t st);
+// phi_bar[g'][c][k] = r[g'][c] (k = 0) + sum_g slgg[g][mat][g'][l(k)] qbar[g][c][k]
+cudaError_t k_adjoint_scatter(const double *r, const double *slgg, const int32_t *mat,
+                              const double *qbar, double *phi_bar, int G, int nmat, int nmom,
+                              int M, long long C, cudaStream_t st);
+// grad[g][c][l] = sum_{k in band l} qbar[g][c][k] flux[g][c][k]
+cudaError_t k_grad_sxs(const double *qbar, const double *flux, double *grad, int G, int nmom,
+                       int M, long long C, cudaStream_t st);
+// out[i] = in[i*M] (moment 0)
+cudaError_t k_moment0(const double *in, double *out, int M, long long n, cudaStream_t st);
+// out[0] = max |a - b|, out[1] = max |a| over n values (as ordered bit patterns
+// of non-negative doubles, combined with atomicMax; out must start at zero)
+cudaError_t k_max_abs_diff(const double *a, const double *b, long long n,
+                           unsigned long long *out, cudaStream_t st);
 cudaError_t k_copy_moment0(const double *flux, double *out, int M, long long n, cudaStream_t st);
 
 }  // namespace snapb200

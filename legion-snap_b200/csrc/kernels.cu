@@ -163,6 +163,79 @@ __global__ void copy_moment0_kernel(const double *__restrict__ flux, double *__r
     out[i * M] = flux[i * M];
 }
 
+// Adjoint of the scattering source (outer.cc:145-171 and inner.cc:130-146
+// transposed): every group, in-group included.
+template <int CELLS>
+__global__ void adjoint_scatter_kernel(const double *__restrict__ r, const double *__restrict__ slgg,
+                                       const int32_t *__restrict__ mat,
+                                       const double *__restrict__ qbar, double *__restrict__ phib,
+                                       int G, int nmat, int nmom, int M, long long C) {
+  extern __shared__ double sq[];   // [G][CELLS][M]
+  const long long ntiles = (C + CELLS - 1) / CELLS;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const long long c0 = tile * CELLS;
+    const int nc = (int)min((long long)CELLS, C - c0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < G * CELLS * M; i += blockDim.x) {
+      const int m = i % M, cc = (i / M) % CELLS, g = i / (M * CELLS);
+      sq[i] = cc < nc ? qbar[((size_t)g * C + c0 + cc) * M + m] : 0.0;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < G * CELLS * M; i += blockDim.x) {
+      const int m = i % M, cc = (i / M) % CELLS, g2 = i / (M * CELLS);
+      if (cc >= nc) continue;
+      const long long c = c0 + cc;
+      const int l = band_of(m), mt = mat[c] - 1;
+      double acc = (m == 0) ? r[(size_t)g2 * C + c] : 0.0;
+      for (int g = 0; g < G; ++g)
+        acc += __ldg(slgg + (((size_t)g * nmat + mt) * G + g2) * nmom + l) *
+               sq[(g * CELLS + cc) * M + m];
+      phib[((size_t)g2 * C + c) * M + m] = acc;
+    }
+  }
+}
+
+__global__ void grad_sxs_kernel(const double *__restrict__ qbar, const double *__restrict__ flux,
+                                double *__restrict__ grad, int G, int nmom, int M, long long C) {
+  const long long n = (long long)G * C * nmom;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int l = (int)(i % nmom);
+    const long long gc = i / nmom;
+    double acc = 0.0;
+    for (int k = l * l; k < (l + 1) * (l + 1) && k < M; ++k) acc += qbar[gc * M + k] * flux[gc * M + k];
+    grad[i] = acc;
+  }
+}
+
+__global__ void moment0_kernel(const double *__restrict__ in, double *__restrict__ out, int M,
+                               long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = in[i * M];
+}
+
+// max |a-b| and max |a| as bit patterns (non-negative doubles order like
+// their unsigned bit patterns); NaN differences count as infinite
+__global__ void max_abs_diff_kernel(const double *__restrict__ a, const double *__restrict__ b,
+                                    long long n, unsigned long long *out) {
+  double md = 0.0, ma = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double d = fabs(a[i] - b[i]);
+    md = (d != d) ? INFINITY : fmax(md, d);
+    ma = fmax(ma, fabs(a[i]));
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    md = fmax(md, __shfl_xor_sync(0xffffffffu, md, o));
+    ma = fmax(ma, __shfl_xor_sync(0xffffffffu, ma, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(out, (unsigned long long)__double_as_longlong(md));
+    atomicMax(out + 1, (unsigned long long)__double_as_longlong(ma));
+  }
+}
+
 __global__ void to_f32_kernel(const double *__restrict__ in, float *__restrict__ out, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
@@ -170,6 +243,38 @@ __global__ void to_f32_kernel(const double *__restrict__ in, float *__restrict__
 }
 
 }  // namespace
+
+cudaError_t k_adjoint_scatter(const double *r, const double *slgg, const int32_t *mat,
+                              const double *qbar, double *phi_bar, int G, int nmat, int nmom,
+                              int M, long long C, cudaStream_t st) {
+  constexpr int CELLS = 4;
+  const size_t smem = sizeof(double) * G * CELLS * M;
+  if (smem > 200 * 1024) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(adjoint_scatter_kernel<CELLS>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const long long tiles = (C + CELLS - 1) / CELLS;
+  adjoint_scatter_kernel<CELLS><<<grid_for(tiles, 1), BLK, smem, st>>>(r, slgg, mat, qbar, phi_bar,
+                                                                        G, nmat, nmom, M, C);
+  return cudaGetLastError();
+}
+
+cudaError_t k_grad_sxs(const double *qbar, const double *flux, double *grad, int G, int nmom,
+                       int M, long long C, cudaStream_t st) {
+  grad_sxs_kernel<<<grid_for((long long)G * C * nmom), BLK, 0, st>>>(qbar, flux, grad, G, nmom, M, C);
+  return cudaGetLastError();
+}
+
+cudaError_t k_moment0(const double *in, double *out, int M, long long n, cudaStream_t st) {
+  moment0_kernel<<<grid_for(n), BLK, 0, st>>>(in, out, M, n);
+  return cudaGetLastError();
+}
+
+cudaError_t k_max_abs_diff(const double *a, const double *b, long long n,
+                           unsigned long long *out, cudaStream_t st) {
+  max_abs_diff_kernel<<<grid_for(n), BLK, 0, st>>>(a, b, n, out);
+  return cudaGetLastError();
+}
 
 cudaError_t k_to_f32(const double *in, float *out, long long n, cudaStream_t st) {
   to_f32_kernel<<<grid_for(n), BLK, 0, st>>>(in, out, n);

@@ -55,6 +55,11 @@ struct snap_ctx {
   size_t wsize = 8;     // bytes per sweep-side word
   // device buffers
   void *d_coef = nullptr, *d_bt1 = nullptr, *d_bt2 = nullptr;
+  void *d_bt1w = nullptr, *d_bt2n = nullptr;   // adjoint tables: ec*w (expansion), ec (accumulation)
+  void *d_pc_store = nullptr;                   // forward state for the adjoint
+  uint8_t *d_flag_store = nullptr;
+  void *d_sbar_slots = nullptr;                 // adjoint of t_xs per octant slot
+  bool state_recorded = false;
   int *d_item_table = nullptr, *d_item_index = nullptr;
   void *d_slots = nullptr, *d_bx = nullptr, *d_by = nullptr;
   int *d_ctrl = nullptr;   // [n_items progress][counter][error][violations]
@@ -78,6 +83,11 @@ void free_ctx(snap_ctx *c) {
   cudaFree(c->d_coef);
   cudaFree(c->d_bt1);
   cudaFree(c->d_bt2);
+  cudaFree(c->d_bt1w);
+  cudaFree(c->d_bt2n);
+  cudaFree(c->d_pc_store);
+  cudaFree(c->d_flag_store);
+  cudaFree(c->d_sbar_slots);
   cudaFree(c->d_item_table);
   cudaFree(c->d_item_index);
   cudaFree(c->d_slots);
@@ -138,6 +148,33 @@ void build_tables(const snap_ctx *c, std::vector<T> &coef, std::vector<double> &
   }
 }
 
+// Adjoint tables: ec*w in the source-expansion layout and ec in the
+// accumulation layout (the roles of the forward tables swapped).
+void build_adjoint_tables(const snap_ctx *c, std::vector<double> &bt1w, std::vector<double> &bt2n) {
+  const int NT = c->shape.NT, MK = c->shape.MK, MN = c->shape.MN, M = c->M, A = c->A;
+  auto ec = [&](int o, int m, int a) { return c->ec[((size_t)o * M + m) * A + a]; };
+  const int B1 = MK * NT * 32, B2 = 2 * NT * MN * 32;
+  bt1w.assign((size_t)8 * B1, 0.0);
+  bt2n.assign((size_t)8 * B2, 0.0);
+  for (int o = 0; o < 8; ++o) {
+    for (int kt = 0; kt < MK; ++kt)
+      for (int nt = 0; nt < NT; ++nt)
+        for (int l = 0; l < 32; ++l) {
+          const int m = (l & 3) * MK + kt, a = 8 * nt + (l >> 2);
+          bt1w[(size_t)o * B1 + (kt * NT + nt) * 32 + l] =
+              (m < M && a < A) ? ec(o, m, a) * c->w[a] : 0.0;
+        }
+    for (int t = 0; t < 2 * NT; ++t)
+      for (int mt = 0; mt < MN; ++mt)
+        for (int l = 0; l < 32; ++l) {
+          const int a = 8 * (t >> 1) + 2 * (l & 3) + (t & 1);
+          const int r = l >> 2;
+          const int m = (r >> 1) * 2 * MN + 2 * mt + (r & 1);
+          bt2n[(size_t)o * B2 + (t * MN + mt) * 32 + l] = (m < M && a < A) ? ec(o, m, a) : 0.0;
+        }
+  }
+}
+
 // Work items of one launch, ordered by tile diagonal, then sweep, then tile:
 // every item's upstream x and y neighbours precede it.
 void build_items(int P, int G, int tx_n, int ty_n, std::vector<int> &table,
@@ -154,7 +191,10 @@ void build_items(int P, int G, int tx_n, int ty_n, std::vector<int> &table,
       }
 }
 
-int sweep_launches(snap_ctx *c, const void *qtot, const void *t_xs, cudaStream_t st) {
+// mode 0: forward sweep; 1: forward sweep recording the state for the
+// adjoint; 2: adjoint sweep (sigma_t adjoint when sbar != null).
+int sweep_launches(snap_ctx *c, const void *qtot, const void *t_xs, cudaStream_t st,
+                   int mode = 0, void *sbar = nullptr) {
   SweepParams p{};
   p.nx = c->cfg.nx;
   p.ny = c->cfg.ny;
@@ -177,15 +217,32 @@ int sweep_launches(snap_ctx *c, const void *qtot, const void *t_xs, cudaStream_t
   p.progress = c->progress();
   p.counter = c->counter();
   p.error = c->error();
-  p.bt1 = c->d_bt1;
-  p.bt2 = c->d_bt2;
+  p.bt1 = mode == 2 ? c->d_bt1w : c->d_bt1;
+  p.bt2 = mode == 2 ? c->d_bt2n : c->d_bt2;
   p.coef = c->d_coef;
+  p.pc_store = mode >= 1 ? c->d_pc_store : nullptr;
+  p.flag_store = mode >= 1 ? c->d_flag_store : nullptr;
+  p.sigt_bar_slots = mode == 2 ? sbar : nullptr;
+  int grid = c->grid;
+  if (mode == 2) {
+    int blocks = 0, sms = 0;
+    size_t smem = 0;
+    if (adjoint_dispatch(c->fp32, c->shape, 1, nullptr, 0, nullptr, &blocks, &smem) != cudaSuccess ||
+        blocks < 1)
+      return fail(SNAP_ERR_UNSUPPORTED, "no adjoint kernel for this shape (8x4 tiles only)");
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+    grid = std::min(blocks * sms, c->n_items);
+  }
   for (int L = 0; L < 8 / c->P; ++L) {
     p.o_base = L * c->P;
     p.accumulate = L > 0;
     SNAP_CUDA(cudaMemsetAsync(c->d_ctrl, 0, sizeof(int) * (c->n_items + 1), st));
-    cudaError_t e = c->fp32 ? launch_sweep_fp32(c->shape, p, c->grid, st)
-                            : launch_sweep_fp64(c->shape, p, c->grid, st);
+    cudaError_t e;
+    if (mode == 2)
+      e = adjoint_dispatch(c->fp32, c->shape, 0, &p, grid, st, nullptr, nullptr);
+    else
+      e = c->fp32 ? launch_sweep_fp32(c->shape, p, grid, st)
+                  : launch_sweep_fp64(c->shape, p, grid, st);
     if (e != cudaSuccess) return cuda_fail(e, "sweep launch");
     ++c->launches;
   }
@@ -302,6 +359,14 @@ int snap_create(const snap_config *cfg, int device, snap_ctx **out) {
     build_tables<double>(c, coef, bt1, bt2);
     if ((rc = upload(&c->d_coef, coef)) || (rc = upload(&c->d_bt1, bt1)) ||
         (rc = upload(&c->d_bt2, bt2))) {
+      free_ctx(c);
+      return rc;
+    }
+  }
+  {
+    std::vector<double> bt1w, bt2n;
+    build_adjoint_tables(c, bt1w, bt2n);
+    if ((rc = upload(&c->d_bt1w, bt1w)) || (rc = upload(&c->d_bt2n, bt2n))) {
       free_ctx(c);
       return rc;
     }
@@ -563,6 +628,218 @@ int snap_transport_solve(snap_ctx *c, const int32_t *mat, const double *qi, cons
 done:
   cleanup();
 #undef STEP
+  return rc;
+}
+
+}  // extern "C"
+
+namespace {
+
+int ensure_state(snap_ctx *c) {
+  if (c->d_pc_store) return SNAP_OK;
+  const size_t n = (size_t)8 * c->cfg.ng * c->C * c->AP;
+  if (cudaMalloc(&c->d_pc_store, n * c->wsize) != cudaSuccess ||
+      cudaMalloc((void **)&c->d_flag_store, n) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(c->d_pc_store);
+    c->d_pc_store = nullptr;
+    return fail(SNAP_ERR_OOM, "cannot allocate the forward-state store for the adjoint");
+  }
+  c->scratch_bytes += n * (c->wsize + 1);
+  return SNAP_OK;
+}
+
+int ensure_sbar(snap_ctx *c) {
+  if (c->d_sbar_slots) return SNAP_OK;
+  const size_t n = (size_t)c->P * c->cfg.ng * c->C;
+  if (cudaMalloc(&c->d_sbar_slots, n * c->wsize) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(SNAP_ERR_OOM, "cannot allocate the sigma_t adjoint slots");
+  }
+  c->scratch_bytes += n * c->wsize;
+  return SNAP_OK;
+}
+
+int adjoint_sweep_impl(snap_ctx *c, const void *phi_bar, const void *t_xs, double *qtot_bar,
+                       double *sigt_bar, cudaStream_t st) {
+  if ((sigt_bar || c->cfg.fixup) && !c->state_recorded)
+    return fail(SNAP_ERR_BAD_ARG, "record the forward state (snap_record_forward) first");
+  int rc;
+  if (sigt_bar && (rc = ensure_sbar(c))) return rc;
+  SNAP_CUDA(cudaEventRecord(c->sw0, st));
+  rc = sweep_launches(c, phi_bar, t_xs, st, 2, sigt_bar ? c->d_sbar_slots : nullptr);
+  if (rc) return rc;
+  SNAP_CUDA(cudaEventRecord(c->sw1, st));
+  SNAP_CUDA(k_reduce_slots(c->d_slots, c->P, c->fp32, qtot_bar, 0, nullptr, c->cfg.ng, c->M, c->C,
+                           0, 0.0, nullptr, st));
+  ++c->launches;
+  if (sigt_bar) {
+    SNAP_CUDA(k_reduce_slots(c->d_sbar_slots, c->P, c->fp32, sigt_bar, 0, nullptr, c->cfg.ng, 1,
+                             c->C, 0, 0.0, nullptr, st));
+    ++c->launches;
+  }
+  return SNAP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int snap_record_forward(snap_ctx *c, const void *qtot, const void *t_xs, void *flux,
+                        void *stream) {
+  if (!c || !qtot || !t_xs || !flux) return fail(SNAP_ERR_BAD_ARG, "null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc = ensure_state(c);
+  if (rc) return rc;
+  SNAP_CUDA(cudaMemsetAsync(c->error(), 0, 2 * sizeof(int), st));
+  rc = sweep_launches(c, qtot, t_xs, st, 1);
+  if (rc) return rc;
+  SNAP_CUDA(k_reduce_slots(c->d_slots, c->P, c->fp32, flux, c->fp32, nullptr, c->cfg.ng, c->M, c->C,
+                           0, 0.0, nullptr, st));
+  ++c->launches;
+  rc = read_ctrl(c, st, nullptr);
+  if (rc == SNAP_OK) c->state_recorded = true;
+  return rc;
+}
+
+int snap_adjoint_sweep(snap_ctx *c, const void *phi_bar, const void *t_xs, double *qtot_bar,
+                       double *sigt_bar, void *stream) {
+  if (!c || !phi_bar || !t_xs || !qtot_bar) return fail(SNAP_ERR_BAD_ARG, "null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  SNAP_CUDA(cudaMemsetAsync(c->error(), 0, 2 * sizeof(int), st));
+  int rc = adjoint_sweep_impl(c, phi_bar, t_xs, qtot_bar, sigt_bar, st);
+  if (rc) return rc;
+  rc = read_ctrl(c, st, nullptr);
+  if (rc == SNAP_OK) account_sweep(c);
+  return rc;
+}
+
+int snap_adjoint_solve(snap_ctx *c, const int32_t *mat, const double *qi, const double *t_xs,
+                       const double *slgg, const double *flux, const double *response,
+                       double *grad_sigt, double *grad_qi, double *grad_sxs, snap_solve_info *info,
+                       void *stream) {
+  if (!c || !mat || !qi || !t_xs || !slgg || !flux || !response || !grad_sigt || !grad_qi || !info)
+    return fail(SNAP_ERR_BAD_ARG, "null argument");
+  if (info->iitm < 1 || info->oitm < 1 || !(info->epsi > 0.0))
+    return fail(SNAP_ERR_BAD_ARG, "iitm, oitm and epsi must be positive");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int G = c->cfg.ng, M = c->M, nmom = c->cfg.nmom;
+  const long long C = c->C, n = (long long)G * C;
+  double *t_xs64 = nullptr, *s_xs = nullptr, *q2grp = nullptr, *qbar = nullptr, *pb = nullptr,
+         *pb2 = nullptr;
+  void *qtot = nullptr, *t_xs_sw = nullptr, *pb_sw = nullptr;
+  unsigned long long *d_norm = nullptr;
+  auto cleanup = [&]() {
+    cudaFree(t_xs64); cudaFree(s_xs); cudaFree(q2grp); cudaFree(qbar); cudaFree(pb);
+    cudaFree(pb2); cudaFree(qtot); cudaFree(d_norm);
+    if (c->fp32) { cudaFree(t_xs_sw); cudaFree(pb_sw); }
+  };
+  if (cudaMalloc(&t_xs64, sizeof(double) * n) != cudaSuccess ||
+      cudaMalloc(&s_xs, sizeof(double) * n * nmom) != cudaSuccess ||
+      cudaMalloc(&q2grp, sizeof(double) * n * M) != cudaSuccess ||
+      cudaMalloc(&qbar, sizeof(double) * n * M) != cudaSuccess ||
+      cudaMalloc(&pb, sizeof(double) * n * M) != cudaSuccess ||
+      cudaMalloc(&pb2, sizeof(double) * n * M) != cudaSuccess ||
+      cudaMalloc(&qtot, c->wsize * n * M) != cudaSuccess ||
+      cudaMalloc((void **)&d_norm, 2 * sizeof(unsigned long long)) != cudaSuccess ||
+      (c->fp32 && cudaMalloc(&t_xs_sw, sizeof(float) * n) != cudaSuccess) ||
+      (c->fp32 && cudaMalloc(&pb_sw, sizeof(float) * n * M) != cudaSuccess)) {
+    cudaGetLastError();
+    cleanup();
+    return fail(SNAP_ERR_OOM, "cannot allocate adjoint solve arrays");
+  }
+  int rc = ensure_state(c);
+  if (rc) {
+    cleanup();
+    return rc;
+  }
+#define ASTEP(x)                \
+  do {                          \
+    cudaError_t e_ = (x);       \
+    if (e_ != cudaSuccess) {    \
+      rc = cuda_fail(e_, #x);   \
+      goto adone;               \
+    }                           \
+  } while (0)
+  {
+    info->inner_total = info->outer_total = info->converged = 0;
+    const double sweep_ms0 = c->sweep_ms;
+    float ms = 0.0f;
+    const int maxit = info->iitm * info->oitm;
+    ASTEP(cudaMemsetAsync(c->error(), 0, 2 * sizeof(int), st));
+    ASTEP(cudaEventRecord(c->ev0, st));
+    // the forward operator at the converged flux: total source
+    ASTEP(cudaMemcpyAsync(t_xs64, t_xs, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    ASTEP(k_expand_scat(slgg, mat, s_xs, G, c->cfg.nmat, nmom, C, st));
+    if (c->fp32) ASTEP(k_to_f32(t_xs64, (float *)t_xs_sw, n, st));
+    ASTEP(k_outer_source(qi, slgg, mat, flux, q2grp, G, c->cfg.nmat, nmom, M, C, st));
+    ASTEP(k_inner_source(s_xs, q2grp, flux, qtot, c->fp32, G, nmom, M, C, st));
+    c->launches += c->fp32 ? 4 : 3;
+    // forward sweep recording the cell-average fluxes and fixup flags
+    rc = sweep_launches(c, qtot, c->fp32 ? t_xs_sw : t_xs64, st, 1);
+    if (rc) goto adone;
+    c->state_recorded = true;
+    // adjoint source iteration: phi_bar = r + S^T M^T L^-T D^T phi_bar,
+    // converged when max|change| <= epsi * max|phi_bar| (the adjoint spans
+    // many decades, so the forward test's per-cell form does not apply)
+    ASTEP(cudaMemsetAsync(qbar, 0, sizeof(double) * n * M, st));
+    ASTEP(k_adjoint_scatter(response, slgg, mat, qbar, pb, G, c->cfg.nmat, nmom, M, C, st));
+    ++c->launches;
+    for (int it = 0; it < maxit; ++it) {
+      const void *src = pb;
+      if (c->fp32) {
+        ASTEP(k_to_f32(pb, (float *)pb_sw, n * M, st));
+        ++c->launches;
+        src = pb_sw;
+      }
+      rc = adjoint_sweep_impl(c, src, c->fp32 ? t_xs_sw : t_xs64, qbar, nullptr, st);
+      if (rc) goto adone;
+      ASTEP(k_adjoint_scatter(response, slgg, mat, qbar, pb2, G, c->cfg.nmat, nmom, M, C, st));
+      ASTEP(cudaMemsetAsync(d_norm, 0, 2 * sizeof(unsigned long long), st));
+      ASTEP(k_max_abs_diff(pb2, pb, n * M, d_norm, st));
+      c->launches += 2;
+      unsigned long long hn[2] = {0, 0};
+      ASTEP(cudaMemcpyAsync(hn, d_norm, sizeof(hn), cudaMemcpyDeviceToHost, st));
+      rc = read_ctrl(c, st, nullptr);
+      if (rc) goto adone;
+      account_sweep(c);
+      std::swap(pb, pb2);
+      ++info->inner_total;
+      double dmax, amax;
+      memcpy(&dmax, &hn[0], sizeof(double));
+      memcpy(&amax, &hn[1], sizeof(double));
+      if (dmax <= info->epsi * amax) {
+        info->converged = 1;
+        break;
+      }
+    }
+    info->outer_total = 1;
+    // gradients from the converged adjoint
+    {
+      const void *src = pb;
+      if (c->fp32) {
+        ASTEP(k_to_f32(pb, (float *)pb_sw, n * M, st));
+        ++c->launches;
+        src = pb_sw;
+      }
+      rc = adjoint_sweep_impl(c, src, c->fp32 ? t_xs_sw : t_xs64, qbar, grad_sigt, st);
+      if (rc) goto adone;
+    }
+    ASTEP(k_moment0(qbar, grad_qi, M, n, st));
+    if (grad_sxs) ASTEP(k_grad_sxs(qbar, flux, grad_sxs, G, nmom, M, C, st));
+    c->launches += grad_sxs ? 2 : 1;
+    rc = read_ctrl(c, st, nullptr);
+    if (rc) goto adone;
+    account_sweep(c);
+    ASTEP(cudaEventRecord(c->ev1, st));
+    ASTEP(cudaEventSynchronize(c->ev1));
+    ASTEP(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    info->total_ms = ms;
+    info->sweep_ms = c->sweep_ms - sweep_ms0;
+  }
+adone:
+  cleanup();
+#undef ASTEP
   return rc;
 }
 

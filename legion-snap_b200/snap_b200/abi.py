@@ -59,6 +59,10 @@ SIGNATURES = {
     "snap_inner_iteration": [_vp, _vp, _vp, _vp, _vp, _vp, C.c_double, _ip, _vp],
     "snap_get_timing": [_vp, C.POINTER(SnapTiming), C.c_int],
     "snap_transport_solve": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, C.POINTER(SnapSolveInfo), _vp],
+    "snap_record_forward": [_vp, _vp, _vp, _vp, _vp],
+    "snap_adjoint_sweep": [_vp, _vp, _vp, _vp, _vp, _vp],
+    "snap_adjoint_solve": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                           C.POINTER(SnapSolveInfo), _vp],
     "snap_sweep_noalloc": [C.POINTER(SnapConfig), _vp, _vp, _vp, _vp],
     "snap_last_error": [],
 }

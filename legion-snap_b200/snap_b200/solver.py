@@ -144,6 +144,78 @@ class Snap:
         return dict(sweep_ms=t.sweep_ms, sweep_calls=t.sweep_calls,
                     kernel_launches=t.kernel_launches)
 
+    # ---- sensitivities ------------------------------------------------------
+    def record_forward(self, qtot, t_xs) -> torch.Tensor:
+        """Forward sweep that also records the state the adjoint needs."""
+        flux = self._empty(self.deck.ng, self.C, self.deck.cmom, dtype=self.sweep_dtype)
+        abi.check(self.lib.snap_record_forward(self.handle, _ptr(qtot), _ptr(t_xs), _ptr(flux),
+                                               _stream()))
+        return flux
+
+    def adjoint_sweep(self, phi_bar, t_xs, with_sigma: bool = False):
+        """qtot_bar = M^T L^-T D^T phi_bar (and the t_xs sensitivity)."""
+        d = self.deck
+        qbar = self._empty(d.ng, self.C, d.cmom)
+        sbar = self._empty(d.ng, self.C) if with_sigma else None
+        abi.check(self.lib.snap_adjoint_sweep(self.handle, _ptr(phi_bar), _ptr(t_xs), _ptr(qbar),
+                                              _ptr(sbar) if sbar is not None else None,
+                                              _stream()))
+        return qbar, sbar
+
+    def adjoint_solve(self, dprob: dict, t_xs: torch.Tensor, flux: torch.Tensor,
+                      response: torch.Tensor, epsi=None, maxit=None) -> dict:
+        """dJ/dt_xs, dJ/dqi and dJ/ds_xs of J = sum response * scalar flux at
+        the converged forward flux (discrete adjoint, fixup flags frozen)."""
+        d = self.deck
+        gs = self._empty(d.ng, self.C)
+        gq = self._empty(d.ng, self.C)
+        gx = self._empty(d.ng, self.C, d.nmom)
+        info = abi.SnapSolveInfo()
+        info.epsi = d.epsi if epsi is None else epsi
+        info.iitm = 1
+        info.oitm = 2000 if maxit is None else maxit
+        abi.check(self.lib.snap_adjoint_solve(
+            self.handle, _ptr(dprob["mat"]), _ptr(dprob["qi"]), _ptr(t_xs.contiguous()),
+            _ptr(dprob["slgg"]), _ptr(flux), _ptr(response.contiguous()), _ptr(gs), _ptr(gq),
+            _ptr(gx), C.byref(info), _stream()))
+        return dict(grad_sigt=gs, grad_qi=gq, grad_sxs=gx, iterations=info.inner_total,
+                    converged=bool(info.converged), total_ms=info.total_ms,
+                    sweep_ms=info.sweep_ms)
+
+    def solve_with_txs(self, dprob: dict, t_xs: torch.Tensor, qi: torch.Tensor,
+                       epsi=None, iitm=None, oitm=None):
+        """The solve loop of snap.cc:472-540 driven from the host through the
+        task-level ABI, with an arbitrary per-cell, per-group t_xs (the
+        reference expands t_xs from material tables; sensitivities need it
+        free).  Returns the flux moments (float64) and the iteration record."""
+        d = self.deck
+        epsi = d.epsi if epsi is None else epsi
+        iitm = d.iitm if iitm is None else iitm
+        oitm = d.oitm if oitm is None else oitm
+        s_xs = self.expand_scattering_cross_section(dprob["slgg"], dprob["mat"])
+        t_sw = t_xs.to(self.sweep_dtype).contiguous()
+        flux = torch.zeros(d.ng, self.C, d.cmom, dtype=torch.float64, device=self.device)
+        qtot = self._empty(d.ng, self.C, d.cmom, dtype=self.sweep_dtype)
+        rec = dict(inner_total=0, outer_total=0, converged=False, inners_per_outer=[])
+        for o in range(oitm):
+            q2 = self.calc_outer_source(qi.contiguous(), dprob["slgg"], dprob["mat"], flux)
+            fpo = flux.clone()
+            conv, inners = False, 0
+            for _ in range(iitm):
+                conv = self.inner_iteration(s_xs, q2, t_sw, flux, qtot, epsi)
+                inners += 1
+                if conv:
+                    break
+            rec["inner_total"] += inners
+            rec["outer_total"] += 1
+            rec["inners_per_outer"].append(inners)
+            if o == 0:
+                continue
+            if conv and self._test(1, flux, fpo, 100.0 * epsi):
+                rec["converged"] = True
+                break
+        return flux, rec
+
     # ---- the solve loop ----------------------------------------------------
     def device_problem(self, prob: dict) -> dict:
         dev = self.device
