@@ -59,6 +59,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-inners", type=int, default=2)
     ap.add_argument("--no-mixed", action="store_true", help="skip the FP32 leg")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint leg")
     ap.add_argument("--groups", type=int, default=None,
                     help="override deck 2's 32 groups (small cases for profiling only)")
     return ap.parse_args()
@@ -355,6 +356,41 @@ def run_snap(args):
             mixed["fp64_inner_iterations"] = rec["inner_total"]
         snap32.close()
 
+    # adjoint cost on the adjoint deck (32^3, 24 angles, 16 groups, nmom 2,
+    # per-cell sigma_t +-10 %): one converged forward solve and one converged
+    # adjoint solve (detector response) to the same tolerance, device time
+    adjoint = None
+    if not args.no_adjoint:
+        d4 = P.deck(4)
+        snap4 = Snap(d4, device=local)
+        dp4 = snap4.device_problem(P.make_problem(d4))
+        r = torch.zeros(d4.ng, d4.nz, d4.ny, d4.nx, dtype=torch.float64, device="cuda")
+        r[:, -4:, -4:, -4:] = (1.0 / torch.arange(1, d4.ng + 1, dtype=torch.float64,
+                                                  device="cuda"))[:, None, None, None]
+        r = r.reshape(d4.ng, d4.cells)
+        eps4 = 1e-6
+        fwd_ms, adj_ms = [], []
+        for _ in range(2):
+            f4, rec4 = snap4.transport_solve(dp4, epsi=eps4, iitm=5, oitm=100)
+            t4 = snap4.expand_cross_section(dp4["sigt"], dp4["mat"]) * dp4["sigt_scale"][None, :]
+            g4 = snap4.adjoint_solve(dp4, t4, f4, r, epsi=eps4)
+            fwd_ms.append(rec4["total_ms"])
+            adj_ms.append(g4["total_ms"])
+        adjoint = {"deck": "32^3 cells, 24 angles/octant, 16 groups, nmom=2, fixup on, "
+                           "detector 4^3 corner box, weights 1/g",
+                   "epsi": eps4, "forward_ms": min(fwd_ms), "adjoint_ms": min(adj_ms),
+                   "adjoint_over_forward": min(adj_ms) / min(fwd_ms),
+                   "forward_inner_iterations": rec4["inner_total"],
+                   "adjoint_iterations": g4["iterations"], "adjoint_converged": g4["converged"],
+                   "note": "forward: per-cell relative test of snap.cc; adjoint: max-norm "
+                           "relative change (the importance spans many decades)"}
+        # per sweep: the adjoint solve runs its iterations plus one recording
+        # forward sweep and one gradient sweep
+        adjoint["adjoint_ms_per_sweep_over_forward_ms_per_inner"] = (
+            (adjoint["adjoint_ms"] / (g4["iterations"] + 2))
+            / (adjoint["forward_ms"] / rec4["inner_total"]))
+        snap4.close()
+
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
@@ -373,6 +409,8 @@ def run_snap(args):
     }
     if mixed is not None:
         line["mixed_precision"] = mixed
+    if adjoint is not None:
+        line["adjoint"] = adjoint
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_reference_sample(d, args.cpu_inners)
         if cb is not None:
