@@ -93,6 +93,17 @@ int snap_calc_outer_source(snap_ctx *ctx, const double *qi, const double *slgg,
                            const int32_t *mat, const double *flux, double *q2grp,
                            void *stream);
 
+/* The outer source of a group shard, for a solve whose energy groups are
+ * split over several contexts (one per GPU): the context's ng groups are
+ * groups g_lo .. g_lo+ng-1 of ng_total.  qi and q2grp hold the shard's groups
+ * ([ng][C] and [ng][C][cmom]); slgg is the full table (ng_total groups) and
+ * flux_all the all-gathered flux of every group ([ng_total][C][cmom]).
+ * Same arithmetic as snap_calc_outer_source (outer.cc:107-217); the
+ * reference has no group sharding (it couples groups through Legion regions). */
+int snap_calc_outer_source_groups(snap_ctx *ctx, int g_lo, int ng_total, const double *qi,
+                                  const double *slgg, const int32_t *mat,
+                                  const double *flux_all, double *q2grp, void *stream);
+
 /* qtot[k] = q2grp[k] + flux[k] * s_xs[l(k)]
  * Replaces CalcInnerSource (inner.cc:163-215 -> run_inner_source_*,
  * gpu_inner.cu:22-117).  FP64 context: qtot double.  FP32 context: qtot float. */

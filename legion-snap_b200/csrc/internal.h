@@ -87,6 +87,9 @@ cudaError_t k_expand_scat(const double *slgg, const int32_t *mat, double *s_xs, 
 cudaError_t k_outer_source(const double *qi, const double *slgg, const int32_t *mat,
                            const double *flux, double *q2grp, int G, int nmat, int nmom, int M,
                            long long C, cudaStream_t st);
+cudaError_t k_outer_source_groups(const double *qi, const double *slgg, const int32_t *mat,
+                                  const double *flux, double *q2grp, int G, int nmat, int nmom,
+                                  int M, long long C, int g_lo, int g_n, cudaStream_t st);
 cudaError_t k_inner_source(const double *s_xs, const double *q2grp, const double *flux,
                            void *qtot, int fp32, int G, int nmom, int M, long long C,
                            cudaStream_t st);

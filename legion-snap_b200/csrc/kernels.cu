@@ -57,11 +57,14 @@ __global__ void expand_scat_kernel(const double *__restrict__ slgg, const int32_
 // outer.cc:107-217 / gpu_outer.cu:22-441, all cmom moments.  A CTA stages
 // the flux of CELLS cells (all groups and moments) in shared memory and
 // produces every (group, cell, moment) output of those cells.
+// Destination groups g_lo .. g_lo+g_n-1 (qi and q2grp hold those groups
+// only); the flux holds all G source groups.
 template <int CELLS>
 __global__ void outer_source_kernel(const double *__restrict__ qi, const double *__restrict__ slgg,
                                     const int32_t *__restrict__ mat,
                                     const double *__restrict__ flux, double *__restrict__ q2grp,
-                                    int G, int nmat, int nmom, int M, long long C) {
+                                    int G, int nmat, int nmom, int M, long long C, int g_lo,
+                                    int g_n) {
   extern __shared__ double sflux[];   // [G][CELLS][M]
   const long long ntiles = (C + CELLS - 1) / CELLS;
   for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -73,18 +76,19 @@ __global__ void outer_source_kernel(const double *__restrict__ qi, const double 
       sflux[i] = cc < nc ? flux[((size_t)g * C + c0 + cc) * M + m] : 0.0;
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < G * CELLS * M; i += blockDim.x) {
-      const int m = i % M, cc = (i / M) % CELLS, g1 = i / (M * CELLS);
+    for (int i = threadIdx.x; i < g_n * CELLS * M; i += blockDim.x) {
+      const int m = i % M, cc = (i / M) % CELLS, gl = i / (M * CELLS);
       if (cc >= nc) continue;
+      const int g1 = g_lo + gl;
       const long long c = c0 + cc;
       const int l = band_of(m);
       const double *row = slgg + ((size_t)g1 * nmat + (mat[c] - 1)) * G * nmom + l;
-      double acc = (m == 0) ? qi[(size_t)g1 * C + c] : 0.0;
+      double acc = (m == 0) ? qi[(size_t)gl * C + c] : 0.0;
       for (int g2 = 0; g2 < G; ++g2) {
         if (g2 == g1) continue;
         acc += __ldg(row + (size_t)g2 * nmom) * sflux[(g2 * CELLS + cc) * M + m];
       }
-      q2grp[((size_t)g1 * C + c) * M + m] = acc;
+      q2grp[((size_t)gl * C + c) * M + m] = acc;
     }
   }
 }
@@ -302,6 +306,12 @@ cudaError_t k_expand_scat(const double *slgg, const int32_t *mat, double *s_xs, 
 cudaError_t k_outer_source(const double *qi, const double *slgg, const int32_t *mat,
                            const double *flux, double *q2grp, int G, int nmat, int nmom, int M,
                            long long C, cudaStream_t st) {
+  return k_outer_source_groups(qi, slgg, mat, flux, q2grp, G, nmat, nmom, M, C, 0, G, st);
+}
+
+cudaError_t k_outer_source_groups(const double *qi, const double *slgg, const int32_t *mat,
+                                  const double *flux, double *q2grp, int G, int nmat, int nmom,
+                                  int M, long long C, int g_lo, int g_n, cudaStream_t st) {
   constexpr int CELLS = 4;
   const size_t smem = sizeof(double) * G * CELLS * M;
   if (smem > 200 * 1024) return cudaErrorInvalidValue;
@@ -310,7 +320,7 @@ cudaError_t k_outer_source(const double *qi, const double *slgg, const int32_t *
   if (e != cudaSuccess) return e;
   const long long tiles = (C + CELLS - 1) / CELLS;
   outer_source_kernel<CELLS><<<grid_for(tiles, 1), BLK, smem, st>>>(qi, slgg, mat, flux, q2grp, G,
-                                                                     nmat, nmom, M, C);
+                                                                     nmat, nmom, M, C, g_lo, g_n);
   return cudaGetLastError();
 }
 

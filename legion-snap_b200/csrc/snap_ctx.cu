@@ -459,6 +459,18 @@ int snap_calc_outer_source(snap_ctx *c, const double *qi, const double *slgg, co
   return SNAP_OK;
 }
 
+int snap_calc_outer_source_groups(snap_ctx *c, int g_lo, int ng_total, const double *qi,
+                                  const double *slgg, const int32_t *mat, const double *flux_all,
+                                  double *q2grp, void *stream) {
+  if (!c || !qi || !slgg || !mat || !flux_all || !q2grp) return fail(SNAP_ERR_BAD_ARG, "null argument");
+  if (g_lo < 0 || ng_total < 1 || g_lo + c->cfg.ng > ng_total)
+    return fail(SNAP_ERR_BAD_ARG, "group range outside the table");
+  SNAP_CUDA(k_outer_source_groups(qi, slgg, mat, flux_all, q2grp, ng_total, c->cfg.nmat,
+                                  c->cfg.nmom, c->M, c->C, g_lo, c->cfg.ng, (cudaStream_t)stream));
+  ++c->launches;
+  return SNAP_OK;
+}
+
 int snap_calc_inner_source(snap_ctx *c, const double *s_xs, const double *q2grp,
                            const double *flux, void *qtot, void *stream) {
   if (!c || !s_xs || !q2grp || !flux || !qtot) return fail(SNAP_ERR_BAD_ARG, "null argument");

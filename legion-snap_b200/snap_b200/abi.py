@@ -53,6 +53,7 @@ SIGNATURES = {
     "snap_expand_xs": [_vp, _vp, _vp, _vp, _vp],
     "snap_expand_scattering_xs": [_vp, _vp, _vp, _vp, _vp],
     "snap_calc_outer_source": [_vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "snap_calc_outer_source_groups": [_vp, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp],
     "snap_calc_inner_source": [_vp, _vp, _vp, _vp, _vp, _vp],
     "snap_sweep": [_vp, _vp, _vp, _vp, _vp],
     "snap_test_convergence": [_vp, C.c_int, _vp, _vp, C.c_double, _ip, _vp],
