@@ -229,6 +229,17 @@ int snap_adjoint_solve(snap_ctx *ctx, const int32_t *mat, const double *qi, cons
 int snap_sweep_noalloc(const snap_config *cfg, const double *qtot, const double *t_xs,
                        double *flux, void *stream);
 
+/* Self-test of the sweep's division arithmetic (no counterpart in the
+ * reference).  The sweep divides by Newton-Raphson refinement of the
+ * hardware reciprocal approximation instead of the correctly rounded
+ * operations; this entry point exposes both for comparison.  For n operand
+ * pairs (a[i], b[i]) in device memory (double for SNAP_FP64, float for
+ * SNAP_FP32) it writes out[4i] = the sweep's 1/b[i], out[4i+1] = the
+ * correctly rounded 1/b[i], out[4i+2] = the sweep's a[i]/b[i] and
+ * out[4i+3] = the correctly rounded a[i]/b[i].  Does not synchronise. */
+int snap_selftest_division(int precision, const void *a, const void *b, long long n, void *out,
+                           void *stream);
+
 /* Last error message of this thread (static storage). */
 const char *snap_last_error(void);
 

@@ -54,4 +54,26 @@ __device__ __forceinline__ bool bounded_wait_geq(const int *flag, int need, int 
   }
 }
 
+// Waits until *flag >= need and returns the last value it read with acquire
+// semantics (>= need on success, so a caller can keep it and skip later waits
+// for smaller needs).  Returns a smaller value when the device error word is
+// set by someone else, or after timeout_ns of device time / a hard iteration
+// cap, in which case it records a timeout in the error word.  Every call ends.
+__device__ __forceinline__ int wait_value_geq(const int *flag, int need, int *err,
+                                              long long timeout_ns, int timeout_code) {
+  int v = ld_acquire_gpu(flag);
+  if (v >= need) return v;
+  const long long t0 = global_timer_ns();
+  for (unsigned spins = 0;; ++spins) {
+    v = ld_acquire_gpu(flag);
+    if (v >= need) return v;
+    if (ld_volatile(err) != 0) return v;
+    if (spins > 32) __nanosleep(spins < 1024 ? 64 : 256);
+    if (global_timer_ns() - t0 > timeout_ns || spins > (1u << 26)) {
+      atomicCAS(err, 0, timeout_code);
+      return v;
+    }
+  }
+}
+
 }  // namespace snapb200

@@ -30,7 +30,7 @@ struct SweepParams {
   void *phi_slots;        // [octants per launch][G][C][M]
   void *bx;               // [item][nz][TY][AP] x-faces leaving a tile
   void *by;               // [item][nz][8][AP]  y-faces leaving a tile
-  int *progress;          // [item] completed steps
+  int *progress;          // completed steps: [item][TY] (forward sweep), [item] (adjoint)
   int *counter;           // work-queue head
   int *error;             // device error word
   const void *bt1;        // [8][MK][NT][32] source-expansion fragments

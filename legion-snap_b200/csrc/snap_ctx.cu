@@ -62,7 +62,7 @@ struct snap_ctx {
   bool state_recorded = false;
   int *d_item_table = nullptr, *d_item_index = nullptr;
   void *d_slots = nullptr, *d_bx = nullptr, *d_by = nullptr;
-  int *d_ctrl = nullptr;   // [n_items progress][counter][error][violations]
+  int *d_ctrl = nullptr;   // [n_items * TY progress][counter][error][violations]
   int *h_ctrl = nullptr;   // pinned: error, violations
   size_t scratch_bytes = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;   // whole-solve timing
@@ -71,9 +71,10 @@ struct snap_ctx {
   long long sweep_calls = 0, launches = 0;
 
   int *progress() { return d_ctrl; }
-  int *counter() { return d_ctrl + n_items; }
-  int *error() { return d_ctrl + n_items + 1; }
-  int *violations() { return d_ctrl + n_items + 2; }
+  size_t n_progress() const { return (size_t)n_items * shape.TY; }
+  int *counter() { return d_ctrl + n_progress(); }
+  int *error() { return d_ctrl + n_progress() + 1; }
+  int *violations() { return d_ctrl + n_progress() + 2; }
 };
 
 namespace {
@@ -236,7 +237,7 @@ int sweep_launches(snap_ctx *c, const void *qtot, const void *t_xs, cudaStream_t
   for (int L = 0; L < 8 / c->P; ++L) {
     p.o_base = L * c->P;
     p.accumulate = L > 0;
-    SNAP_CUDA(cudaMemsetAsync(c->d_ctrl, 0, sizeof(int) * (c->n_items + 1), st));
+    SNAP_CUDA(cudaMemsetAsync(c->d_ctrl, 0, sizeof(int) * (c->n_progress() + 1), st));
     cudaError_t e;
     if (mode == 2)
       e = adjoint_dispatch(c->fp32, c->shape, 0, &p, grid, st, nullptr, nullptr);
@@ -399,13 +400,13 @@ int snap_create(const snap_config *cfg, int device, snap_ctx **out) {
   const size_t by_b = (size_t)c->n_items * cfg->nz * 8 * c->AP * c->wsize;
   if (cudaMalloc(&c->d_slots, slots_b) != cudaSuccess || cudaMalloc(&c->d_bx, bx_b) != cudaSuccess ||
       cudaMalloc(&c->d_by, by_b) != cudaSuccess ||
-      cudaMalloc((void **)&c->d_ctrl, sizeof(int) * (c->n_items + 3)) != cudaSuccess) {
+      cudaMalloc((void **)&c->d_ctrl, sizeof(int) * (c->n_progress() + 3)) != cudaSuccess) {
     cudaGetLastError();
     free_ctx(c);
     return fail(SNAP_ERR_OOM, "cannot allocate sweep scratch");
   }
-  c->scratch_bytes = slots_b + bx_b + by_b + sizeof(int) * (c->n_items + 3);
-  if (cudaMemset(c->d_ctrl, 0, sizeof(int) * (c->n_items + 3)) != cudaSuccess ||
+  c->scratch_bytes = slots_b + bx_b + by_b + sizeof(int) * (c->n_progress() + 3);
+  if (cudaMemset(c->d_ctrl, 0, sizeof(int) * (c->n_progress() + 3)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_ctrl, 4 * sizeof(int)) != cudaSuccess ||
       cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
       cudaEventCreate(&c->sw0) != cudaSuccess || cudaEventCreate(&c->sw1) != cudaSuccess) {

@@ -1,6 +1,10 @@
 // Entry points of the sweep kernels: shape dispatch over the per-precision,
 // per-angle-tile translation units (the kernel itself is in sweep.cuh).
+#include "snap_b200.h"
 #include "sweep.cuh"
+
+#include <algorithm>
+#include <string>
 
 namespace snapb200 {
 namespace {
@@ -61,3 +65,38 @@ size_t sweep_fp32_smem(const SweepShape &sh) {
 }
 
 }  // namespace snapb200
+
+namespace {
+
+template <typename T>
+__global__ void division_selftest_kernel(const T *a, const T *b, long long n, T *out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    out[4 * i] = snapb200::sw::recip(b[i]);
+    out[4 * i + 1] = snapb200::sw::recip_rn(b[i]);
+    out[4 * i + 2] = snapb200::sw::divide(a[i], b[i]);
+    out[4 * i + 3] = snapb200::sw::div_rn(a[i], b[i]);
+  }
+}
+
+}  // namespace
+
+extern "C" int snap_selftest_division(int precision, const void *a, const void *b, long long n,
+                                      void *out, void *stream) {
+  if (!a || !b || !out || n < 0 || (precision != SNAP_FP64 && precision != SNAP_FP32))
+    return snapb200::set_last_error(SNAP_ERR_BAD_ARG, "snap_selftest_division: bad argument");
+  if (n == 0) return SNAP_OK;
+  const int grid = (int)std::min<long long>((n + 255) / 256, 4096);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (precision == SNAP_FP64)
+    division_selftest_kernel<double><<<grid, 256, 0, st>>>((const double *)a, (const double *)b,
+                                                           n, (double *)out);
+  else
+    division_selftest_kernel<float><<<grid, 256, 0, st>>>((const float *)a, (const float *)b, n,
+                                                          (float *)out);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return snapb200::set_last_error(SNAP_ERR_CUDA, std::string("snap_selftest_division: ") +
+                                                       cudaGetErrorString(e));
+  return SNAP_OK;
+}

@@ -146,7 +146,8 @@ extern "C" int snap_sweep_noalloc(const snap_config *cfg, const double *qtot, co
   const size_t o_by = take(sizeof(double) * (size_t)n_items * cfg->nz * 8 * AP);
   const size_t o_tab = take(sizeof(int) * (size_t)n_items);
   const size_t o_idx = take(sizeof(int) * (size_t)n_items);
-  const size_t o_ctl = take(sizeof(int) * ((size_t)n_items + 2));   // progress, counter, error
+  const size_t n_prog = (size_t)n_items * sh.TY;   // completed steps per (item, warp)
+  const size_t o_ctl = take(sizeof(int) * (n_prog + 2));   // progress, counter, error
   if (off > SNAP_NOALLOC_SCRATCH_BYTES)
     return fail(SNAP_ERR_UNSUPPORTED,
                 "problem needs " + std::to_string(off) + " bytes of sweep scratch; the static limit "
@@ -213,8 +214,8 @@ extern "C" int snap_sweep_noalloc(const snap_config *cfg, const double *qtot, co
   p.bx = base + o_bx;
   p.by = base + o_by;
   p.progress = ctl;
-  p.counter = ctl + n_items;
-  p.error = ctl + n_items + 1;
+  p.counter = ctl + n_prog;
+  p.error = ctl + n_prog + 1;
   p.bt1 = base + o_bt1;
   p.bt2 = base + o_bt2;
   p.coef = base + o_coef;
@@ -222,7 +223,7 @@ extern "C" int snap_sweep_noalloc(const snap_config *cfg, const double *qtot, co
   for (int oct = 0; oct < 8; ++oct) {
     p.o_base = oct;
     p.accumulate = oct > 0;
-    NA_CUDA(cudaMemsetAsync(ctl, 0, sizeof(int) * ((size_t)n_items + 1), st));
+    NA_CUDA(cudaMemsetAsync(ctl, 0, sizeof(int) * (n_prog + 1), st));
     NA_CUDA(launch_sweep_fp64(sh, p, grid, st));
   }
   int err = 0;

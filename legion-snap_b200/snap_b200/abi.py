@@ -65,6 +65,7 @@ SIGNATURES = {
     "snap_adjoint_solve": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                            C.POINTER(SnapSolveInfo), _vp],
     "snap_sweep_noalloc": [C.POINTER(SnapConfig), _vp, _vp, _vp, _vp],
+    "snap_selftest_division": [C.c_int, _vp, _vp, C.c_longlong, _vp, _vp],
     "snap_last_error": [],
 }
 
