@@ -52,6 +52,7 @@ struct SweepShape {
   int MK;   // source k-tiles of 4 moments (0: single moment)
   int MN;   // moment n-tiles of 8
   int TY;   // warps per CTA = tile rows in y
+  int KT;   // moment tiles of 8 of the split-TF32 FP32 kernel (0: single moment)
 };
 
 // Records the message snap_last_error() returns; returns `code`.
@@ -72,6 +73,13 @@ cudaError_t launch_sweep_fp32(const SweepShape &sh, const SweepParams &p, int gr
 cudaError_t sweep_fp32_occupancy(const SweepShape &sh, int *blocks_per_sm, size_t *smem);
 size_t sweep_fp32_smem(const SweepShape &sh);
 bool sweep_fp32_supported(const SweepShape &sh);
+
+// FP32 sweep on the TF32 tensor cores (sweep_tc.cuh): work items are
+// (octant, group pair, tile), fragment tables from build_tc_tables
+bool sweep_tc32_supported(const SweepShape &sh);
+cudaError_t launch_sweep_tc32(const SweepShape &sh, const SweepParams &p, int grid,
+                              cudaStream_t st);
+cudaError_t sweep_tc32_occupancy(const SweepShape &sh, int *blocks_per_sm, size_t *smem);
 
 // adjoint sweep kernels (adjoint_dispatch.cu); op 0 launch, 1 occupancy, 2 smem
 bool adjoint_supported(const SweepShape &sh);

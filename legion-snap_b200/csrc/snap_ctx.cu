@@ -61,6 +61,11 @@ struct snap_ctx {
   void *d_sbar_slots = nullptr;                 // adjoint of t_xs per octant slot
   bool state_recorded = false;
   int *d_item_table = nullptr, *d_item_index = nullptr;
+  // FP32 contexts: the split-TF32 tensor-core sweep over group pairs
+  int tc32 = 0;
+  int n_pair_items = 0, grid_tc = 0;
+  int *d_pair_table = nullptr, *d_pair_index = nullptr;
+  void *d_tc1 = nullptr, *d_tc2 = nullptr;
   void *d_slots = nullptr, *d_bx = nullptr, *d_by = nullptr;
   int *d_ctrl = nullptr;   // [n_items * TY progress][counter][error][violations]
   int *h_ctrl = nullptr;   // pinned: error, violations
@@ -71,7 +76,7 @@ struct snap_ctx {
   long long sweep_calls = 0, launches = 0;
 
   int *progress() { return d_ctrl; }
-  size_t n_progress() const { return (size_t)n_items * shape.TY; }
+  size_t n_progress() const { return (size_t)std::max(n_items, n_pair_items) * shape.TY; }
   int *counter() { return d_ctrl + n_progress(); }
   int *error() { return d_ctrl + n_progress() + 1; }
   int *violations() { return d_ctrl + n_progress() + 2; }
@@ -91,6 +96,10 @@ void free_ctx(snap_ctx *c) {
   cudaFree(c->d_sbar_slots);
   cudaFree(c->d_item_table);
   cudaFree(c->d_item_index);
+  cudaFree(c->d_pair_table);
+  cudaFree(c->d_pair_index);
+  cudaFree(c->d_tc1);
+  cudaFree(c->d_tc2);
   cudaFree(c->d_slots);
   cudaFree(c->d_bx);
   cudaFree(c->d_by);
@@ -147,6 +156,56 @@ void build_tables(const snap_ctx *c, std::vector<T> &coef, std::vector<double> &
               (m < M && a < A) ? ec(o, m, a) * c->w[a] : 0.0;
         }
   }
+}
+
+// x rounded to TF32 (10 explicit mantissa bits), to nearest with ties away
+// from zero: add half of the dropped 13-bit field to the magnitude, truncate.
+uint32_t tf32_bits(float x) {
+  uint32_t u;
+  std::memcpy(&u, &x, 4);
+  if ((u & 0x7f800000u) == 0x7f800000u) return u;   // inf / nan unchanged
+  return (u + 0x1000u) & 0xffffe000u;
+}
+float from_bits(uint32_t u) {
+  float x;
+  std::memcpy(&x, &u, 4);
+  return x;
+}
+// {hi(b0), hi(b1), lo(b0), lo(b1)}: each value split into two TF32 parts
+void put_split(uint32_t *dst, double b0, double b1) {
+  const float f0 = (float)b0, f1 = (float)b1;
+  const uint32_t h0 = tf32_bits(f0), h1 = tf32_bits(f1);
+  dst[0] = h0;
+  dst[1] = h1;
+  dst[2] = tf32_bits(f0 - from_bits(h0));
+  dst[3] = tf32_bits(f1 - from_bits(h1));
+}
+
+// Fragment tables of the split-TF32 FP32 sweep (m16n8k8 B operands, lane
+// l = 4g + t, uint4 per lane):
+//   source  [8][KT][NT][32]: ec[m][a] at k = moments 8kt + 2t, 8kt + 2t + 1
+//           and n = angle 8nt + g;
+//   moments [8][NT][KT][32]: ec[m][a] w[a] at k = angles 8nt + 2t, 8nt + 2t + 1
+//           and n = moment 8mt + g.
+void build_tc_tables(const snap_ctx *c, std::vector<uint32_t> &tc1, std::vector<uint32_t> &tc2) {
+  const int NT = c->shape.NT, KT = c->shape.KT, M = c->M, A = c->A;
+  auto ec = [&](int o, int m, int a) {
+    return (m < M && a < A) ? c->ec[((size_t)o * M + m) * A + a] : 0.0;
+  };
+  auto ecw = [&](int o, int m, int a) { return (m < M && a < A) ? ec(o, m, a) * c->w[a] : 0.0; };
+  const size_t F = (size_t)KT * NT * 32 * 4;
+  tc1.assign(8 * F, 0u);
+  tc2.assign(8 * F, 0u);
+  for (int o = 0; o < 8; ++o)
+    for (int kt = 0; kt < KT; ++kt)
+      for (int nt = 0; nt < NT; ++nt)
+        for (int l = 0; l < 32; ++l) {
+          const int g = l >> 2, t = l & 3;
+          put_split(&tc1[o * F + (((size_t)kt * NT + nt) * 32 + l) * 4],
+                    ec(o, 8 * kt + 2 * t, 8 * nt + g), ec(o, 8 * kt + 2 * t + 1, 8 * nt + g));
+          put_split(&tc2[o * F + (((size_t)nt * KT + kt) * 32 + l) * 4],
+                    ecw(o, 8 * kt + g, 8 * nt + 2 * t), ecw(o, 8 * kt + g, 8 * nt + 2 * t + 1));
+        }
 }
 
 // Adjoint tables: ec*w in the source-expansion layout and ec in the
@@ -225,6 +284,15 @@ int sweep_launches(snap_ctx *c, const void *qtot, const void *t_xs, cudaStream_t
   p.flag_store = mode >= 1 ? c->d_flag_store : nullptr;
   p.sigt_bar_slots = mode == 2 ? sbar : nullptr;
   int grid = c->grid;
+  const bool tc = c->tc32 && mode != 2;
+  if (tc) {
+    p.n_items = c->n_pair_items;
+    p.item_table = c->d_pair_table;
+    p.item_index = c->d_pair_index;
+    p.bt1 = c->d_tc1;
+    p.bt2 = c->d_tc2;
+    grid = c->grid_tc;
+  }
   if (mode == 2) {
     int blocks = 0, sms = 0;
     size_t smem = 0;
@@ -241,6 +309,8 @@ int sweep_launches(snap_ctx *c, const void *qtot, const void *t_xs, cudaStream_t
     cudaError_t e;
     if (mode == 2)
       e = adjoint_dispatch(c->fp32, c->shape, 0, &p, grid, st, nullptr, nullptr);
+    else if (tc)
+      e = launch_sweep_tc32(c->shape, p, grid, st);
     else
       e = c->fp32 ? launch_sweep_fp32(c->shape, p, grid, st)
                   : launch_sweep_fp64(c->shape, p, grid, st);
@@ -329,6 +399,7 @@ int snap_create(const snap_config *cfg, int device, snap_ctx **out) {
   c->shape.MK = c->M == 1 ? 0 : (c->M + 3) / 4;
   c->shape.MN = c->shape.MK == 0 ? 0 : (c->shape.MK + 1) / 2;
   c->shape.TY = tile_y;
+  c->shape.KT = c->M == 1 ? 0 : (c->M + 7) / 8;
   c->AP = 8 * c->shape.NT;
   c->wsize = c->fp32 ? sizeof(float) : sizeof(double);
   const bool ok = c->fp32 ? sweep_fp32_supported(c->shape) : sweep_fp64_supported(c->shape);
@@ -338,6 +409,8 @@ int snap_create(const snap_config *cfg, int device, snap_ctx **out) {
   }
   c->tiles_x = cfg->nx / 8;
   c->tiles_y = cfg->ny / c->shape.TY;
+  // FP32 contexts sweep on the TF32 tensor cores unless told otherwise
+  c->tc32 = c->fp32 && sweep_tc32_supported(c->shape) && !getenv("SNAP_B200_FP32_DMMA");
 
   int rc;
   cudaError_t e = cudaSetDevice(device);
@@ -354,6 +427,14 @@ int snap_create(const snap_config *cfg, int device, snap_ctx **out) {
         (rc = upload(&c->d_bt2, bt2))) {
       free_ctx(c);
       return rc;
+    }
+    if (c->tc32) {
+      std::vector<uint32_t> tc1, tc2;
+      build_tc_tables(c, tc1, tc2);
+      if ((rc = upload(&c->d_tc1, tc1)) || (rc = upload(&c->d_tc2, tc2))) {
+        free_ctx(c);
+        return rc;
+      }
     }
   } else {
     std::vector<double> coef, bt1, bt2;
@@ -377,8 +458,9 @@ int snap_create(const snap_config *cfg, int device, snap_ctx **out) {
   cudaMemGetInfo(&free_b, &total_b);
   const size_t budget = (size_t)(0.55 * (double)free_b);
   const int G = cfg->ng;
+  const int G_faces = c->tc32 ? 2 * ((G + 1) / 2) : G;   // group pairs carry a phantom member
   auto scratch_for = [&](int P) {
-    const size_t items = (size_t)P * G * c->tiles_x * c->tiles_y;
+    const size_t items = (size_t)P * G_faces * c->tiles_x * c->tiles_y;
     return (size_t)P * G * c->C * c->M * c->wsize +
            items * (size_t)cfg->nz * (c->shape.TY + 8) * c->AP * c->wsize;
   };
@@ -395,9 +477,20 @@ int snap_create(const snap_config *cfg, int device, snap_ctx **out) {
     free_ctx(c);
     return rc;
   }
+  if (c->tc32) {
+    build_items(P, (G + 1) / 2, c->tiles_x, c->tiles_y, table, index);
+    c->n_pair_items = (int)table.size();
+    if ((rc = upload((void **)&c->d_pair_table, table)) ||
+        (rc = upload((void **)&c->d_pair_index, index))) {
+      free_ctx(c);
+      return rc;
+    }
+  }
   const size_t slots_b = (size_t)P * G * c->C * c->M * c->wsize;
-  const size_t bx_b = (size_t)c->n_items * cfg->nz * c->shape.TY * c->AP * c->wsize;
-  const size_t by_b = (size_t)c->n_items * cfg->nz * 8 * c->AP * c->wsize;
+  // tile-edge faces: per item of one group, or of one group pair (two groups)
+  const size_t face_items = std::max((size_t)c->n_items, (size_t)2 * c->n_pair_items);
+  const size_t bx_b = face_items * cfg->nz * c->shape.TY * c->AP * c->wsize;
+  const size_t by_b = face_items * cfg->nz * 8 * c->AP * c->wsize;
   if (cudaMalloc(&c->d_slots, slots_b) != cudaSuccess || cudaMalloc(&c->d_bx, bx_b) != cudaSuccess ||
       cudaMalloc(&c->d_by, by_b) != cudaSuccess ||
       cudaMalloc((void **)&c->d_ctrl, sizeof(int) * (c->n_progress() + 3)) != cudaSuccess) {
@@ -424,6 +517,14 @@ int snap_create(const snap_config *cfg, int device, snap_ctx **out) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   c->grid = std::min(blocks * sms, c->n_items);
   if (const char *ge = getenv("SNAP_B200_GRID")) c->grid = std::max(1, std::min(atoi(ge), c->grid));
+  if (c->tc32) {
+    e = sweep_tc32_occupancy(c->shape, &blocks, &smem);
+    if (e != cudaSuccess || blocks < 1) {
+      free_ctx(c);
+      return fail(SNAP_ERR_UNSUPPORTED, "FP32 tensor-core sweep kernel does not fit on the device");
+    }
+    c->grid_tc = std::min(blocks * sms, c->n_pair_items);
+  }
   *out = c;
   return SNAP_OK;
 }

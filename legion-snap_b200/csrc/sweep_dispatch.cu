@@ -2,6 +2,7 @@
 // per-angle-tile translation units (the kernel itself is in sweep.cuh).
 #include "snap_b200.h"
 #include "sweep.cuh"
+#include "sweep_tc.cuh"
 
 #include <algorithm>
 #include <string>
@@ -21,6 +22,12 @@ const DispatchFn kFp32[9] = {nullptr,
                              sweep_fp32_dispatch_nt3, sweep_fp32_dispatch_nt4,
                              sweep_fp32_dispatch_nt5, sweep_fp32_dispatch_nt6,
                              sweep_fp32_dispatch_nt7, sweep_fp32_dispatch_nt8};
+
+using TcFn = cudaError_t (*)(int, int, const SweepParams *, int, cudaStream_t, int *, size_t *);
+const TcFn kTc32[9] = {nullptr,
+                       sweep_tc32_dispatch_nt1, sweep_tc32_dispatch_nt2, sweep_tc32_dispatch_nt3,
+                       sweep_tc32_dispatch_nt4, sweep_tc32_dispatch_nt5, sweep_tc32_dispatch_nt6,
+                       sweep_tc32_dispatch_nt7, sweep_tc32_dispatch_nt8};
 
 bool supported(const SweepShape &sh) {
   return (sh.TY == 8 || sh.TY == 4) && sh.NT >= 1 && sh.NT <= 8 && sh.MK >= 0 && sh.MK <= 4;
@@ -44,6 +51,19 @@ cudaError_t launch_sweep_fp64(const SweepShape &sh, const SweepParams &p, int gr
 cudaError_t launch_sweep_fp32(const SweepShape &sh, const SweepParams &p, int grid,
                               cudaStream_t st) {
   return dispatch(kFp32, sh, 0, &p, grid, st, nullptr, nullptr);
+}
+
+bool sweep_tc32_supported(const SweepShape &sh) {
+  return sh.TY == 4 && sh.NT >= 1 && sh.NT <= 8 && sh.KT >= 0 && sh.KT <= 2;
+}
+cudaError_t launch_sweep_tc32(const SweepShape &sh, const SweepParams &p, int grid,
+                              cudaStream_t st) {
+  if (!sweep_tc32_supported(sh)) return cudaErrorInvalidValue;
+  return kTc32[sh.NT](sh.KT, 0, &p, grid, st, nullptr, nullptr);
+}
+cudaError_t sweep_tc32_occupancy(const SweepShape &sh, int *blocks_per_sm, size_t *smem) {
+  if (!sweep_tc32_supported(sh)) return cudaErrorInvalidValue;
+  return kTc32[sh.NT](sh.KT, 1, nullptr, 0, nullptr, blocks_per_sm, smem);
 }
 
 cudaError_t sweep_fp64_occupancy(const SweepShape &sh, int *blocks_per_sm, size_t *smem) {
