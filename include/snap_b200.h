@@ -93,6 +93,18 @@ int snap_calc_outer_source(snap_ctx *ctx, const double *qi, const double *slgg,
                            const int32_t *mat, const double *flux, double *q2grp,
                            void *stream);
 
+/* The same outer source with the group-to-group contraction on the BF16
+ * tensor cores: both operands split into two BF16 parts (three products,
+ * FP32 accumulation), relative error of order 1e-5 of the scattering term;
+ * qi is added in FP64.  Replaces CalcOuterSource (outer.cc:220-284) where a
+ * low-precision source is acceptable: snap_transport_solve uses it in FP32
+ * contexts only while the outer iteration is far from converged.
+ * SNAP_ERR_UNSUPPORTED when the group count needs more shared memory than a
+ * CTA has (about 300 groups). */
+int snap_calc_outer_source_tc(snap_ctx *ctx, const double *qi, const double *slgg,
+                              const int32_t *mat, const double *flux, double *q2grp,
+                              void *stream);
+
 /* The outer source of a group shard, for a solve whose energy groups are
  * split over several contexts (one per GPU): the context's ng groups are
  * groups g_lo .. g_lo+ng-1 of ng_total.  qi and q2grp hold the shard's groups
@@ -159,13 +171,21 @@ typedef struct {
   int inners_per_outer[1024];
   double sweep_ms;     /* device time spent in the sweep kernels */
   double total_ms;     /* device time of the whole solve */
+  int outers_lowp;     /* outer iterations whose source came from the BF16 tensor cores */
 } snap_solve_info;
 
 /* Full steady-state fixed-source solve, the sequential semantics of the
  * reference's predicated loop (snap.cc:409-541): cross-section expansion,
  * outer source, inner source, sweep, inner/outer convergence.  flux (cmom
  * moments, double) holds the result; it is zeroed first (snap.cc:313-316).
- * Replaces Snap::transport_solve's loop body for one time step. */
+ * Replaces Snap::transport_solve's loop body for one time step.
+ * FP32 contexts (the precision form) take the outer source from
+ * snap_calc_outer_source_tc while the last outer iteration changed some
+ * scalar flux by more than 1000*epsi relative (ten times the outer
+ * convergence tolerance), and from the FP64 source after that; convergence
+ * is only declared on an outer iteration with the FP64 source, so the
+ * solution is the fixed point of the FP64 source (set
+ * SNAP_B200_FP32_EXACT_OUTER=1 to use the FP64 source throughout). */
 int snap_transport_solve(snap_ctx *ctx, const int32_t *mat, const double *qi,
                          const double *sigt, const double *slgg, const double *sigt_scale,
                          double *flux, snap_solve_info *info, void *stream);

@@ -98,6 +98,13 @@ cudaError_t k_outer_source(const double *qi, const double *slgg, const int32_t *
 cudaError_t k_outer_source_groups(const double *qi, const double *slgg, const int32_t *mat,
                                   const double *flux, double *q2grp, int G, int nmat, int nmom,
                                   int M, long long C, int g_lo, int g_n, cudaStream_t st);
+// outer source with the group-to-group contraction on the BF16 tensor cores
+// (outer_tc.cu); `tab` holds outer_tc_table_words() words of scratch
+size_t outer_tc_table_words(int G, int nmat, int nmom);
+size_t outer_tc_smem_bytes(int G, int nmat, int nmom);
+cudaError_t k_outer_source_tc(const double *qi, const double *slgg, const int32_t *mat,
+                              const double *flux, double *q2grp, uint32_t *tab, int G, int nmat,
+                              int nmom, int M, long long C, cudaStream_t st);
 cudaError_t k_inner_source(const double *s_xs, const double *q2grp, const double *flux,
                            void *qtot, int fp32, int G, int nmom, int M, long long C,
                            cudaStream_t st);

@@ -66,6 +66,7 @@ struct snap_ctx {
   int n_pair_items = 0, grid_tc = 0;
   int *d_pair_table = nullptr, *d_pair_index = nullptr;
   void *d_tc1 = nullptr, *d_tc2 = nullptr;
+  uint32_t *d_scat_tc = nullptr;   // BF16 scattering fragments of the tensor-core outer source
   void *d_slots = nullptr, *d_bx = nullptr, *d_by = nullptr;
   int *d_ctrl = nullptr;   // [n_items * TY progress][counter][error][violations]
   int *h_ctrl = nullptr;   // pinned: error, violations
@@ -100,6 +101,7 @@ void free_ctx(snap_ctx *c) {
   cudaFree(c->d_pair_index);
   cudaFree(c->d_tc1);
   cudaFree(c->d_tc2);
+  cudaFree(c->d_scat_tc);
   cudaFree(c->d_slots);
   cudaFree(c->d_bx);
   cudaFree(c->d_by);
@@ -409,8 +411,11 @@ int snap_create(const snap_config *cfg, int device, snap_ctx **out) {
   }
   c->tiles_x = cfg->nx / 8;
   c->tiles_y = cfg->ny / c->shape.TY;
-  // FP32 contexts sweep on the TF32 tensor cores unless told otherwise
-  c->tc32 = c->fp32 && sweep_tc32_supported(c->shape) && !getenv("SNAP_B200_FP32_DMMA");
+  // FP32 contexts can sweep with the contractions on the TF32 tensor cores
+  // (group pairs); measured slower than the FP64-tensor-core contractions on
+  // the 64^3 deck, so it is opt-in
+  c->tc32 = c->fp32 && sweep_tc32_supported(c->shape) && getenv("SNAP_B200_FP32_TC") &&
+            atoi(getenv("SNAP_B200_FP32_TC")) != 0;
 
   int rc;
   cudaError_t e = cudaSetDevice(device);
@@ -561,6 +566,25 @@ int snap_calc_outer_source(snap_ctx *c, const double *qi, const double *slgg, co
   return SNAP_OK;
 }
 
+int snap_calc_outer_source_tc(snap_ctx *c, const double *qi, const double *slgg,
+                              const int32_t *mat, const double *flux, double *q2grp, void *stream) {
+  if (!c || !qi || !slgg || !mat || !flux || !q2grp) return fail(SNAP_ERR_BAD_ARG, "null argument");
+  if (outer_tc_smem_bytes(c->cfg.ng, c->cfg.nmat, c->cfg.nmom) > 200 * 1024 || c->cfg.nmat > 32)
+    return fail(SNAP_ERR_UNSUPPORTED, "too many groups or materials for the tensor-core outer source");
+  if (!c->d_scat_tc) {
+    const size_t words = outer_tc_table_words(c->cfg.ng, c->cfg.nmat, c->cfg.nmom);
+    if (cudaMalloc((void **)&c->d_scat_tc, sizeof(uint32_t) * words) != cudaSuccess) {
+      cudaGetLastError();
+      c->d_scat_tc = nullptr;
+      return fail(SNAP_ERR_OOM, "cannot allocate the tensor-core scattering table");
+    }
+  }
+  SNAP_CUDA(k_outer_source_tc(qi, slgg, mat, flux, q2grp, c->d_scat_tc, c->cfg.ng, c->cfg.nmat,
+                              c->cfg.nmom, c->M, c->C, (cudaStream_t)stream));
+  c->launches += 2;
+  return SNAP_OK;
+}
+
 int snap_calc_outer_source_groups(snap_ctx *c, int g_lo, int ng_total, const double *qi,
                                   const double *slgg, const int32_t *mat, const double *flux_all,
                                   double *q2grp, void *stream) {
@@ -681,7 +705,7 @@ int snap_transport_solve(snap_ctx *c, const int32_t *mat, const double *qi, cons
     }                           \
   } while (0)
   {
-    info->inner_total = info->outer_total = info->converged = 0;
+    info->inner_total = info->outer_total = info->converged = info->outers_lowp = 0;
     info->sweep_ms = info->total_ms = 0.0;
     const double sweep_ms0 = c->sweep_ms;
     float ms = 0.0f;
@@ -702,10 +726,27 @@ int snap_transport_solve(snap_ctx *c, const int32_t *mat, const double *qi, cons
       ++c->launches;
     }
     STEP(cudaMemsetAsync(flux, 0, sizeof(double) * n * M, st));   // snap.cc:313-316
+    // precision form: BF16 tensor-core outer source while far from convergence
+    const bool lowp = c->fp32 && !(getenv("SNAP_B200_FP32_EXACT_OUTER") &&
+                                   atoi(getenv("SNAP_B200_FP32_EXACT_OUTER")) != 0) &&
+                      outer_tc_smem_bytes(G, c->cfg.nmat, nmom) <= 200 * 1024 && c->cfg.nmat <= 32;
+    // outer change above which the low-precision source is used: ten times
+    // the outer convergence tolerance, so the outer iterations that can
+    // converge run on the FP64 source
+    const double kFar = 1000.0 * info->epsi;
+    bool far = true;
     for (int o = 0; o < info->oitm; ++o) {
-      STEP(k_outer_source(qi, slgg, mat, flux, q2grp, G, c->cfg.nmat, nmom, M, C, st));
+      const bool use_tc = lowp && far && o > 0;   // outer 0 has zero flux: q2 = qi exactly
+      if (use_tc) {
+        rc = snap_calc_outer_source_tc(c, qi, slgg, mat, flux, q2grp, st);
+        if (rc) goto done;
+        ++info->outers_lowp;
+      } else {
+        STEP(k_outer_source(qi, slgg, mat, flux, q2grp, G, c->cfg.nmat, nmom, M, C, st));
+        ++c->launches;
+      }
       STEP(k_copy_moment0(flux, fpo, M, n, st));                   // save_fluxes -> flux0po
-      c->launches += 2;
+      ++c->launches;
       bool inner_conv = false;
       int inners = 0;
       for (int i = 0; i < info->iitm; ++i) {
@@ -720,7 +761,18 @@ int snap_transport_solve(snap_ctx *c, const int32_t *mat, const double *qi, cons
       if (o < 1024) info->inners_per_outer[o] = inners;
       ++info->outer_total;
       if (o == 0) continue;                                        // snap.cc:521-522
-      if (inner_conv) {
+      if (lowp && far) {
+        // FP64 outer residual: every scalar flux within kFar of the last outer?
+        STEP(cudaMemsetAsync(c->violations(), 0, sizeof(int), st));
+        STEP(k_count_violations(flux, fpo, M, n, kFar, c->violations(), st));
+        ++c->launches;
+        int v = 0;
+        rc = read_ctrl(c, st, &v);
+        if (rc) goto done;
+        if (v == 0) far = false;
+      }
+      // convergence only on an outer iteration with the FP64 source
+      if (inner_conv && !use_tc) {
         STEP(cudaMemsetAsync(c->violations(), 0, sizeof(int), st));
         STEP(k_count_violations(flux, fpo, M, n, 100.0 * info->epsi, c->violations(), st));
         ++c->launches;
@@ -876,7 +928,7 @@ int snap_adjoint_solve(snap_ctx *c, const int32_t *mat, const double *qi, const 
     }                           \
   } while (0)
   {
-    info->inner_total = info->outer_total = info->converged = 0;
+    info->inner_total = info->outer_total = info->converged = info->outers_lowp = 0;
     const double sweep_ms0 = c->sweep_ms;
     float ms = 0.0f;
     const int maxit = info->iitm * info->oitm;

@@ -30,7 +30,7 @@ class SnapSolveInfo(C.Structure):
     _fields_ = [("epsi", C.c_double), ("iitm", C.c_int), ("oitm", C.c_int),
                 ("inner_total", C.c_int), ("outer_total", C.c_int), ("converged", C.c_int),
                 ("inners_per_outer", C.c_int * 1024), ("sweep_ms", C.c_double),
-                ("total_ms", C.c_double)]
+                ("total_ms", C.c_double), ("outers_lowp", C.c_int)]
 
 
 class SnapTiming(C.Structure):
@@ -53,6 +53,7 @@ SIGNATURES = {
     "snap_expand_xs": [_vp, _vp, _vp, _vp, _vp],
     "snap_expand_scattering_xs": [_vp, _vp, _vp, _vp, _vp],
     "snap_calc_outer_source": [_vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "snap_calc_outer_source_tc": [_vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "snap_calc_outer_source_groups": [_vp, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp],
     "snap_calc_inner_source": [_vp, _vp, _vp, _vp, _vp, _vp],
     "snap_sweep": [_vp, _vp, _vp, _vp, _vp],

@@ -104,6 +104,14 @@ class Snap:
                                                   _ptr(flux), _ptr(q2), _stream()))
         return q2
 
+    def calc_outer_source_tc(self, qi, slgg, mat, flux) -> torch.Tensor:
+        """The outer source with the group-to-group contraction on the BF16
+        tensor cores (split operands, FP32 accumulation)."""
+        q2 = self._empty(self.deck.ng, self.C, self.deck.cmom)
+        abi.check(self.lib.snap_calc_outer_source_tc(self.handle, _ptr(qi), _ptr(slgg), _ptr(mat),
+                                                     _ptr(flux), _ptr(q2), _stream()))
+        return q2
+
     def calc_inner_source(self, s_xs, q2grp, flux) -> torch.Tensor:
         qtot = self._empty(self.deck.ng, self.C, self.deck.cmom, dtype=self.sweep_dtype)
         abi.check(self.lib.snap_calc_inner_source(self.handle, _ptr(s_xs), _ptr(q2grp),
@@ -248,5 +256,5 @@ class Snap:
         rec = dict(inner_total=info.inner_total, outer_total=info.outer_total,
                    converged=bool(info.converged),
                    inners_per_outer=list(info.inners_per_outer[:info.outer_total]),
-                   total_ms=info.total_ms, sweep_ms=info.sweep_ms)
+                   total_ms=info.total_ms, sweep_ms=info.sweep_ms, outers_lowp=info.outers_lowp)
         return flux, rec

@@ -284,3 +284,74 @@ def test_fp32_solve_error(d):
     snap = snap_ctx32(d)
     flux, rec = snap.transport_solve(snap.device_problem(prob))
     assert rel_err(flux[..., 0].cpu().numpy(), ref[..., 0]) < FP32_TOL
+
+
+# ------------------------------------- FP32 form, TF32 tensor-core contractions
+@pytest.fixture
+def tf32_sweep(monkeypatch):
+    """Contexts created inside the test sweep with the split-TF32 kernel
+    (group pairs on the m16n8k8 TF32 MMA)."""
+    monkeypatch.setenv("SNAP_B200_FP32_TC", "1")
+
+
+@pytest.mark.parametrize("d", [P.deck(1), P.Deck(16, 16, 16, nang=36, ng=3, nmom=4),
+                               P.Deck(16, 16, 8, nang=20, ng=4, nmom=3)],
+                         ids=["deck1", "A36_cmom16_odd_groups", "cmom9"])
+def test_fp32_tf32_sweep_error(d, tf32_sweep):
+    prob = P.make_problem(d)
+    o = Oracle(d)
+    t_xs, _ = o.expand(prob)
+    qtot = random_qtot(d, 12)
+    ref = o.sweep(qtot, t_xs)
+    got = snap_ctx32(d).mini_kba_sweep(dev(qtot).float(), dev(t_xs).float()).double().cpu().numpy()
+    assert rel_err(got[..., 0], ref[..., 0]) < FP32_TOL
+    assert moment_err(got, ref) < FP32_TOL
+
+
+def test_fp32_tf32_solve_error(tf32_sweep):
+    d = P.Deck(16, 16, 16, nang=12, ng=5, nmom=4, epsi=1e-6, iitm=3, oitm=4)
+    prob = P.make_problem(d)
+    ref, _ = Oracle(d).solve(prob)
+    snap = snap_ctx32(d)
+    flux, rec = snap.transport_solve(snap.device_problem(prob))
+    assert rel_err(flux[..., 0].cpu().numpy(), ref[..., 0]) < FP32_TOL
+
+
+# --------------------------------- outer source on the BF16 tensor cores
+@pytest.mark.parametrize("d", [P.Deck(16, 16, 16, nang=4, ng=20, nmom=4),
+                               P.Deck(16, 16, 8, nang=4, ng=4, nmom=1),
+                               P.Deck(16, 16, 8, nang=4, ng=33, nmom=3)],
+                         ids=["G20_cmom16", "G4_cmom1", "G33_cmom9"])
+def test_outer_source_tc_matches_fp64(d):
+    """The split-BF16 tensor-core outer source against the FP64 one (itself at
+    1e-12 of the oracle): the scattering term within 1e-4 of its largest
+    magnitude per moment, the fixed source exact, on tiles that mix the two
+    materials and group counts that are not multiples of 16."""
+    snap = snap_ctx(d)
+    dp = snap.device_problem(P.make_problem(d))
+    flux = dev(random_qtot(d, 5))
+    ref = snap.calc_outer_source(dp["qi"], dp["slgg"], dp["mat"], flux)
+    got = snap.calc_outer_source_tc(dp["qi"], dp["slgg"], dp["mat"], flux)
+    scat_ref = ref.clone()
+    scat_ref[..., 0] -= dp["qi"]
+    scat_got = got.clone()
+    scat_got[..., 0] -= dp["qi"]
+    err = moment_err(scat_got.cpu().numpy(), scat_ref.cpu().numpy())
+    assert err < 1e-4, err
+    assert err > 0.0   # it is the low-precision path
+
+
+def test_fp32_solve_refines_lowp_source():
+    """An FP32 solve takes its early outer sources from the tensor cores and
+    still lands within 1e-5 of the FP64 oracle: the last outer iterations use
+    the FP64 source."""
+    d = P.Deck(16, 16, 16, nang=12, ng=6, nmom=2, epsi=1e-6, iitm=3, oitm=30)
+    prob = P.make_problem(d)
+    ref, _ = Oracle(d).solve(prob)
+    from snap_b200.solver import Snap
+    snap = Snap(d, precision="fp32")
+    flux, rec = snap.transport_solve(snap.device_problem(prob))
+    assert rec["converged"]
+    assert rec["outers_lowp"] >= 1
+    assert rec["outers_lowp"] < rec["outer_total"]
+    assert rel_err(flux[..., 0].cpu().numpy(), ref[..., 0]) < FP32_TOL
