@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-inners", type=int, default=2)
     ap.add_argument("--no-mixed", action="store_true", help="skip the FP32 leg")
+    ap.add_argument("--no-mixed-large", action="store_true",
+                    help="skip the mixed-precision leg on the 128^3, 64-group deck")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint leg")
     ap.add_argument("--groups", type=int, default=None,
                     help="override deck 2's 32 groups (small cases for profiling only)")
@@ -219,6 +221,74 @@ def run_reference(args):
     return 0
 
 
+MIXED_PRECISION = ("fp32 sweep (moment contractions on FP64 tensor cores); group-to-group "
+                   "outer source on BF16 tensor cores (split operands, fp32 accumulation) while "
+                   "some scalar flux changes by more than 1000*epsi per outer, fp64 source for "
+                   "the final outers; fp64 octant sums, inner sources and convergence")
+
+
+def outer_source_times(snap, snap32, dp, flux, reps=5):
+    """Device time of one outer source: FP64 kernel against the BF16
+    tensor-core kernel, on the same flux."""
+    import torch
+    out = {}
+    for name, fn in (("fp64_ms", snap.calc_outer_source), ("bf16_tc_ms", snap32.calc_outer_source_tc)):
+        fn(dp["qi"], dp["slgg"], dp["mat"], flux)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            fn(dp["qi"], dp["slgg"], dp["mat"], flux)
+        e1.record()
+        torch.cuda.synchronize()
+        out[name] = e0.elapsed_time(e1) / reps
+    out["speedup"] = out["fp64_ms"] / out["bf16_tc_ms"]
+    return out
+
+
+def mixed_large_deck(local):
+    """The mixed-precision configuration at 128^3 cells, 48 angles, 64 groups,
+    nmom 4: FP32 inner-iteration grind time against FP64, whole-solve times
+    and the scalar-flux error of the FP32 solve against the FP64 solve."""
+    import torch
+
+    from snap_b200 import problem as P
+    from snap_b200.solver import Snap
+    d = P.deck(3)
+    prob = P.make_problem(d)
+    res = {"deck": "128^3 cells, 48 angles/octant, 64 groups, nmom=4 (16 moments), fixup on",
+           "units_per_sweep": d.units_per_sweep}
+    try:
+        phi = {}
+        for prec in ("fp64", "fp32"):
+            snap = Snap(d, precision=prec, device=local)
+            dp = snap.device_problem(prob)
+            flux, rec = snap.transport_solve(dp)
+            phi[prec] = flux[..., 0].clone()
+            res[prec] = {"solve_ms": rec["total_ms"], "inner_iterations": rec["inner_total"],
+                         "outer_iterations": rec["outer_total"], "converged": rec["converged"],
+                         "sweep_ms": rec["sweep_ms"] / max(rec["inner_total"], 1),
+                         "grind_ns": rec["sweep_ms"] / max(rec["inner_total"], 1) * 1e6
+                                     / d.units_per_sweep,
+                         "sweep_scratch_gb": snap.scratch_bytes / 1e9}
+            if prec == "fp32":
+                res[prec]["outers_lowp_source"] = rec["outers_lowp"]
+            del flux, dp
+            snap.close()
+            del snap
+            torch.cuda.empty_cache()
+        diff = (phi["fp32"] - phi["fp64"]).abs() / phi["fp64"].abs().clamp_min(1e-300)
+        res["max_rel_err_scalar_flux"] = float(diff.max())
+        res["rms_rel_err_scalar_flux"] = float(diff.pow(2).mean().sqrt())
+        res["frac_values_above_1e-5"] = float((diff > 1e-5).double().mean())
+        res["sweep_speedup_fp32_vs_fp64"] = res["fp64"]["sweep_ms"] / res["fp32"]["sweep_ms"]
+        res["solve_speedup_fp32_vs_fp64"] = res["fp64"]["solve_ms"] / res["fp32"]["solve_ms"]
+    except Exception as e:   # report, do not lose the main bench line
+        res["error"] = f"{type(e).__name__}: {e}"
+    return res
+
+
 def run_snap(args):
     import torch
     import torch.distributed as dist
@@ -338,8 +408,7 @@ def run_snap(args):
         ms32 = ev0.elapsed_time(ev1) / args.steps
         tm32 = snap32.timing()
         sweep32 = tm32["sweep_ms"] / max(tm32["sweep_calls"], 1)
-        mixed = {"precision": "fp32 sweep (moment contractions on FP64 tensor cores), "
-                              "fp64 octant sums, sources, convergence",
+        mixed = {"precision": MIXED_PRECISION,
                  "value": ms32 * 1e6 / d.units_per_sweep, "unit": UNIT, "ms_per_step": ms32,
                  "speedup_vs_fp64": ms_per_step / ms32, "sweep_ms": sweep32,
                  "roofline": {"bound": "hbm", "bytes_per_unit": (3 * d.cmom + 1) * 4 / d.nang,
@@ -354,7 +423,16 @@ def run_snap(args):
             mixed["rms_rel_err_scalar_flux"] = float(diff.pow(2).mean().sqrt())
             mixed["inner_iterations"] = rec32["inner_total"]
             mixed["fp64_inner_iterations"] = rec["inner_total"]
+            mixed["outers_lowp_source"] = rec32["outers_lowp"]
+            mixed["outer_iterations"] = rec32["outer_total"]
+            mixed["solve_ms"] = rec32["total_ms"]
+            mixed["fp64_solve_ms"] = rec["total_ms"]
+            mixed["solve_speedup_vs_fp64"] = rec["total_ms"] / rec32["total_ms"]
+        mixed["outer_source"] = outer_source_times(snap, snap32, dp, flux)
         snap32.close()
+        if not args.no_mixed_large:
+            del snap32, qtot32, flux32, q2grp32
+            mixed["large_deck"] = mixed_large_deck(local)
 
     # adjoint cost on the adjoint deck (32^3, 24 angles, 16 groups, nmom 2,
     # per-cell sigma_t +-10 %): one converged forward solve and one converged

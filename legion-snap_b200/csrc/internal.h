@@ -109,10 +109,12 @@ cudaError_t k_inner_source(const double *s_xs, const double *q2grp, const double
                            void *qtot, int fp32, int G, int nmom, int M, long long C,
                            cudaStream_t st);
 // flux = sum of `slots` partial slots; optionally counts convergence violations
-// of the new scalar flux against the old one (read before it is overwritten).
+// of the new scalar flux against the old one (read before it is overwritten)
+// and records the largest relative change (float bits, atomicMax) in *maxdf.
 cudaError_t k_reduce_slots(const void *slots, int nslots, int fp32, void *flux_out,
                            int out_fp32, double *flux64_out, int G, int M, long long C,
-                           int test, double epsi, int *violations, cudaStream_t st);
+                           int test, double epsi, int *violations, cudaStream_t st,
+                           unsigned *maxdf = nullptr);
 cudaError_t k_count_violations(const double *flux, const double *prev, int M, long long n,
                                double epsi, int *violations, cudaStream_t st);
 cudaError_t k_to_f32(const double *in, float *out, long long n, cudaStream_t st);

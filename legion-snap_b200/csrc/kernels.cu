@@ -114,9 +114,10 @@ __global__ void inner_source_kernel(const double *__restrict__ s_xs,
 template <typename ST, typename OT>
 __global__ void reduce_slots_kernel(const ST *__restrict__ slots, int nslots, OT *flux_out,
                                     double *flux64_out, int G, int M, long long C, int test,
-                                    double epsi, int *violations) {
+                                    double epsi, int *violations, unsigned *maxdf) {
   const long long n = (long long)G * C * M;
   int bad = 0;
+  float dmax = 0.0f;   // largest relative change seen by this thread
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     double s = 0.0;
@@ -130,6 +131,7 @@ __global__ void reduce_slots_kernel(const ST *__restrict__ slots, int nslots, OT
       }
       df = fabs(s / prev - df);
       if (df > epsi) ++bad;
+      dmax = fmaxf(dmax, (float)df);   // NaN compares false: ignored, as in the count
     }
     if (flux_out) flux_out[i] = (OT)s;
     if (flux64_out && (void *)flux64_out != (void *)flux_out) flux64_out[i] = s;
@@ -137,6 +139,10 @@ __global__ void reduce_slots_kernel(const ST *__restrict__ slots, int nslots, OT
   if (test) {
     bad = __reduce_add_sync(0xffffffffu, bad);
     if ((threadIdx.x & 31) == 0 && bad) atomicAdd(violations, bad);
+    if (maxdf) {   // non-negative floats order like their bit patterns
+      const unsigned m = __reduce_max_sync(0xffffffffu, __float_as_uint(dmax));
+      if ((threadIdx.x & 31) == 0 && m) atomicMax(maxdf, m);
+    }
   }
 }
 
@@ -337,20 +343,21 @@ cudaError_t k_inner_source(const double *s_xs, const double *q2grp, const double
 
 cudaError_t k_reduce_slots(const void *slots, int nslots, int fp32, void *flux_out, int out_fp32,
                            double *flux64_out, int G, int M, long long C, int test, double epsi,
-                           int *violations, cudaStream_t st) {
+                           int *violations, cudaStream_t st, unsigned *maxdf) {
   const int grid = grid_for((long long)G * C * M);
   if (fp32) {
     if (out_fp32)
       reduce_slots_kernel<float, float><<<grid, BLK, 0, st>>>(
-          (const float *)slots, nslots, (float *)flux_out, flux64_out, G, M, C, test, epsi, violations);
+          (const float *)slots, nslots, (float *)flux_out, flux64_out, G, M, C, test, epsi,
+          violations, maxdf);
     else
       reduce_slots_kernel<float, double><<<grid, BLK, 0, st>>>(
           (const float *)slots, nslots, (double *)flux_out, flux64_out, G, M, C, test, epsi,
-          violations);
+          violations, maxdf);
   } else {
     reduce_slots_kernel<double, double><<<grid, BLK, 0, st>>>(
         (const double *)slots, nslots, (double *)flux_out, flux64_out, G, M, C, test, epsi,
-        violations);
+        violations, maxdf);
   }
   return cudaGetLastError();
 }

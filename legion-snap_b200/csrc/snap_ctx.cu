@@ -69,7 +69,8 @@ struct snap_ctx {
   uint32_t *d_scat_tc = nullptr;   // BF16 scattering fragments of the tensor-core outer source
   void *d_slots = nullptr, *d_bx = nullptr, *d_by = nullptr;
   int *d_ctrl = nullptr;   // [n_items * TY progress][counter][error][violations]
-  int *h_ctrl = nullptr;   // pinned: error, violations
+  int *h_ctrl = nullptr;   // pinned: error, violations, largest change (float bits)
+  float prev_inner_df = 0.0f;   // FP32 contexts: largest change of the previous inner iteration
   size_t scratch_bytes = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;   // whole-solve timing
   cudaEvent_t sw0 = nullptr, sw1 = nullptr;   // sweep timing
@@ -81,6 +82,7 @@ struct snap_ctx {
   int *counter() { return d_ctrl + n_progress(); }
   int *error() { return d_ctrl + n_progress() + 1; }
   int *violations() { return d_ctrl + n_progress() + 2; }
+  unsigned *maxdf() { return (unsigned *)(d_ctrl + n_progress() + 3); }
 };
 
 namespace {
@@ -331,7 +333,7 @@ int timed_sweep(snap_ctx *c, const void *qtot, const void *t_xs, void *flux, int
   if (rc) return rc;
   SNAP_CUDA(cudaEventRecord(c->sw1, st));
   SNAP_CUDA(k_reduce_slots(c->d_slots, c->P, c->fp32, flux, flux_fp32, flux64, c->cfg.ng, c->M,
-                           c->C, test, epsi, c->violations(), st));
+                           c->C, test, epsi, c->violations(), st, test ? c->maxdf() : nullptr));
   ++c->launches;
   return SNAP_OK;
 }
@@ -346,7 +348,7 @@ void account_sweep(snap_ctx *c) {
 
 // Reads the device error word and the violation counter (synchronises).
 int read_ctrl(snap_ctx *c, cudaStream_t st, int *violations) {
-  SNAP_CUDA(cudaMemcpyAsync(c->h_ctrl, c->error(), 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+  SNAP_CUDA(cudaMemcpyAsync(c->h_ctrl, c->error(), 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
   SNAP_CUDA(cudaStreamSynchronize(st));
   if (c->h_ctrl[0] == DEV_ERR_TIMEOUT)
     return fail(SNAP_ERR_DEVICE_TIMEOUT, "a sweep tile waited past its limit for an upstream tile");
@@ -498,13 +500,13 @@ int snap_create(const snap_config *cfg, int device, snap_ctx **out) {
   const size_t by_b = face_items * cfg->nz * 8 * c->AP * c->wsize;
   if (cudaMalloc(&c->d_slots, slots_b) != cudaSuccess || cudaMalloc(&c->d_bx, bx_b) != cudaSuccess ||
       cudaMalloc(&c->d_by, by_b) != cudaSuccess ||
-      cudaMalloc((void **)&c->d_ctrl, sizeof(int) * (c->n_progress() + 3)) != cudaSuccess) {
+      cudaMalloc((void **)&c->d_ctrl, sizeof(int) * (c->n_progress() + 4)) != cudaSuccess) {
     cudaGetLastError();
     free_ctx(c);
     return fail(SNAP_ERR_OOM, "cannot allocate sweep scratch");
   }
-  c->scratch_bytes = slots_b + bx_b + by_b + sizeof(int) * (c->n_progress() + 3);
-  if (cudaMemset(c->d_ctrl, 0, sizeof(int) * (c->n_progress() + 3)) != cudaSuccess ||
+  c->scratch_bytes = slots_b + bx_b + by_b + sizeof(int) * (c->n_progress() + 4);
+  if (cudaMemset(c->d_ctrl, 0, sizeof(int) * (c->n_progress() + 4)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_ctrl, 4 * sizeof(int)) != cudaSuccess ||
       cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
       cudaEventCreate(&c->sw0) != cudaSuccess || cudaEventCreate(&c->sw1) != cudaSuccess) {
@@ -622,7 +624,7 @@ int snap_inner_iteration(snap_ctx *c, const double *s_xs, const double *q2grp, c
   if (!c || !s_xs || !q2grp || !t_xs || !flux || !qtot || !converged)
     return fail(SNAP_ERR_BAD_ARG, "null argument");
   cudaStream_t st = (cudaStream_t)stream;
-  SNAP_CUDA(cudaMemsetAsync(c->error(), 0, 2 * sizeof(int), st));
+  SNAP_CUDA(cudaMemsetAsync(c->error(), 0, 3 * sizeof(int), st));
   SNAP_CUDA(k_inner_source(s_xs, q2grp, flux, qtot, c->fp32, c->cfg.ng, c->cfg.nmom, c->M, c->C,
                            st));
   ++c->launches;
@@ -638,6 +640,16 @@ int snap_inner_iteration(snap_ctx *c, const double *s_xs, const double *q2grp, c
   if (rc) return rc;
   account_sweep(c);
   *converged = v == 0;
+  if (c->fp32) {
+    // FP32 contexts also stop an inner loop that has stagnated at the FP32
+    // rounding level: the largest change stopped falling (at least halving
+    // per inner away from it) while below 2^-15 relative
+    float df = 0.0f;
+    std::memcpy(&df, &c->h_ctrl[2], sizeof(float));
+    if (c->prev_inner_df > 0.0f && df <= 0x1p-15f && df >= 0.5f * c->prev_inner_df)
+      *converged = 1;
+    c->prev_inner_df = df;
+  }
   return SNAP_OK;
 }
 
@@ -742,6 +754,7 @@ int snap_transport_solve(snap_ctx *c, const int32_t *mat, const double *qi, cons
     bool far = true;
     for (int o = 0; o < info->oitm; ++o) {
       const bool use_tc = lowp && far && o > 0;   // outer 0 has zero flux: q2 = qi exactly
+      c->prev_inner_df = 0.0f;                     // no stagnation test on an outer's first inner
       if (use_tc) {
         rc = snap_calc_outer_source_tc(c, qi, slgg, mat, flux, q2grp, st);
         if (rc) goto done;
