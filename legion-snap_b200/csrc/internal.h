@@ -21,6 +21,7 @@ struct SweepParams {
   int n_items;     // work items of this launch
   int o_base;      // first octant of this launch
   int accumulate;  // add into the flux slots instead of storing
+  int atomic_flux; // phi_slots is the FP64 flux [G][C][M]: every octant adds into it atomically
   int fixup;
   long long timeout_ns;
   const int *item_table;  // item -> (sweep << 16) | (tx << 8) | ty
@@ -105,6 +106,16 @@ size_t outer_tc_smem_bytes(int G, int nmat, int nmom);
 cudaError_t k_outer_source_tc(const double *qi, const double *slgg, const int32_t *mat,
                               const double *flux, double *q2grp, uint32_t *tab, int G, int nmat,
                               int nmom, int M, long long C, cudaStream_t st);
+// qtot as k_inner_source, and in the same pass the old scalar flux saved to
+// old0[g*C + c] and the flux moments cleared (for sweeps that add octants
+// straight into the flux)
+cudaError_t k_inner_source_save(const double *s_xs, const double *q2grp, double *flux, void *qtot,
+                                int fp32, double *old0, int G, int nmom, int M, long long C,
+                                cudaStream_t st);
+// inner test of the new scalar flux flux[i*M] against old0[i]: violation
+// count and the largest relative change (float bits)
+cudaError_t k_test_change(const double *flux, const double *old0, int M, long long n, double epsi,
+                          int *violations, unsigned *maxdf, cudaStream_t st);
 cudaError_t k_inner_source(const double *s_xs, const double *q2grp, const double *flux,
                            void *qtot, int fp32, int G, int nmom, int M, long long C,
                            cudaStream_t st);

@@ -108,6 +108,48 @@ __global__ void inner_source_kernel(const double *__restrict__ s_xs,
   }
 }
 
+// inner source with the old scalar flux saved and the moments cleared
+template <typename QT>
+__global__ void inner_source_save_kernel(const double *__restrict__ s_xs,
+                                         const double *__restrict__ q2grp, double *flux,
+                                         QT *__restrict__ qtot, double *__restrict__ old0, int G,
+                                         int nmom, int M, long long C) {
+  const long long n = (long long)G * C * M;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int m = (int)(i % M);
+    const long long gc = i / M;
+    const double f = flux[i];
+    qtot[i] = (QT)(q2grp[i] + f * s_xs[gc * nmom + band_of(m)]);
+    if (m == 0) old0[gc] = f;
+    flux[i] = 0.0;
+  }
+}
+
+// inner.cc:283-324 against a saved scalar flux, with the largest change
+__global__ void test_change_kernel(const double *__restrict__ flux, const double *__restrict__ old0,
+                                   int M, long long n, double epsi, int *violations,
+                                   unsigned *maxdf) {
+  int bad = 0;
+  float dmax = 0.0f;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    double p = old0[i];
+    double df = 1.0;
+    if (fabs(p) < 1.0e-12) {
+      p = 1.0;
+      df = 0.0;
+    }
+    df = fabs(flux[i * M] / p - df);
+    if (df > epsi) ++bad;
+    dmax = fmaxf(dmax, (float)df);
+  }
+  bad = __reduce_add_sync(0xffffffffu, bad);
+  if ((threadIdx.x & 31) == 0 && bad) atomicAdd(violations, bad);
+  const unsigned m = __reduce_max_sync(0xffffffffu, __float_as_uint(dmax));
+  if ((threadIdx.x & 31) == 0 && m) atomicMax(maxdf, m);
+}
+
 // flux = sum of the octant slots.  With `test`, also the inner convergence
 // test of inner.cc:283-324 against the previous scalar flux, which is read
 // from flux64_out before it is overwritten.
@@ -338,6 +380,25 @@ cudaError_t k_inner_source(const double *s_xs, const double *q2grp, const double
   else
     inner_source_kernel<double><<<grid, BLK, 0, st>>>(s_xs, q2grp, flux, (double *)qtot, G, nmom, M,
                                                       C);
+  return cudaGetLastError();
+}
+
+cudaError_t k_inner_source_save(const double *s_xs, const double *q2grp, double *flux, void *qtot,
+                                int fp32, double *old0, int G, int nmom, int M, long long C,
+                                cudaStream_t st) {
+  const int grid = grid_for((long long)G * C * M);
+  if (fp32)
+    inner_source_save_kernel<float><<<grid, BLK, 0, st>>>(s_xs, q2grp, flux, (float *)qtot, old0, G,
+                                                          nmom, M, C);
+  else
+    inner_source_save_kernel<double><<<grid, BLK, 0, st>>>(s_xs, q2grp, flux, (double *)qtot, old0,
+                                                           G, nmom, M, C);
+  return cudaGetLastError();
+}
+
+cudaError_t k_test_change(const double *flux, const double *old0, int M, long long n, double epsi,
+                          int *violations, unsigned *maxdf, cudaStream_t st) {
+  test_change_kernel<<<grid_for(n), BLK, 0, st>>>(flux, old0, M, n, epsi, violations, maxdf);
   return cudaGetLastError();
 }
 
