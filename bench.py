@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--no-mixed", action="store_true", help="skip the FP32 leg")
     ap.add_argument("--no-mixed-large", action="store_true",
                     help="skip the mixed-precision leg on the 128^3, 64-group deck")
+    ap.add_argument("--no-memory-deck", action="store_true",
+                    help="skip the FP32 forward solve on the 192^3, 64-group, nmom 3 deck")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint leg")
     ap.add_argument("--groups", type=int, default=None,
                     help="override deck 2's 32 groups (small cases for profiling only)")
@@ -289,6 +291,49 @@ def mixed_large_deck(local):
     return res
 
 
+def memory_pressure_deck(local):
+    """FP32 forward solve of the 192^3 cells, 48 angles, 64 groups, nmom 3
+    deck with a seeded random 50 % material mix in the central 96^3 block,
+    one octant per sweep launch (the device holds about 140 GB for it).  The
+    FP64 solve of this deck does not fit beside it, so the error is not
+    measured here; the 128^3 deck carries the error comparison."""
+    import torch
+
+    from snap_b200 import problem as P
+    from snap_b200.solver import Snap
+    d = P.deck(5)
+    res = {"deck": "192^3 cells, 48 angles/octant, 64 groups, nmom=3 (9 moments), random 50% "
+                   "material mix in the central 96^3 block, fixup on, FP32 sweep",
+           "units_per_sweep": d.units_per_sweep}
+    old = os.environ.get("SNAP_B200_OCTANTS_PER_LAUNCH")
+    os.environ["SNAP_B200_OCTANTS_PER_LAUNCH"] = "1"
+    try:
+        snap = Snap(d, precision="fp32", device=local)
+        dp = snap.device_problem(P.make_problem(d))
+        flux, rec = snap.transport_solve(dp)
+        free, total = torch.cuda.mem_get_info()
+        res.update({"solve_ms": rec["total_ms"], "inner_iterations": rec["inner_total"],
+                    "outer_iterations": rec["outer_total"], "converged": rec["converged"],
+                    "outers_lowp_source": rec["outers_lowp"],
+                    "sweep_ms": rec["sweep_ms"] / max(rec["inner_total"], 1),
+                    "grind_ns": rec["sweep_ms"] / max(rec["inner_total"], 1) * 1e6 / d.units_per_sweep,
+                    "scalar_flux_positive_finite": bool(torch.isfinite(flux).all()
+                                                        and (flux[..., 0] > 0).all()),
+                    "device_gb_in_use_after_solve": (total - free) / 1e9})
+        del flux, dp
+        snap.close()
+        del snap
+        torch.cuda.empty_cache()
+    except Exception as e:   # report, do not lose the main bench line
+        res["error"] = f"{type(e).__name__}: {e}"
+    finally:
+        if old is None:
+            os.environ.pop("SNAP_B200_OCTANTS_PER_LAUNCH", None)
+        else:
+            os.environ["SNAP_B200_OCTANTS_PER_LAUNCH"] = old
+    return res
+
+
 def run_snap(args):
     import torch
     import torch.distributed as dist
@@ -430,9 +475,11 @@ def run_snap(args):
             mixed["solve_speedup_vs_fp64"] = rec["total_ms"] / rec32["total_ms"]
         mixed["outer_source"] = outer_source_times(snap, snap32, dp, flux)
         snap32.close()
+        del snap32, qtot32, flux32, q2grp32
         if not args.no_mixed_large:
-            del snap32, qtot32, flux32, q2grp32
             mixed["large_deck"] = mixed_large_deck(local)
+        if not args.no_memory_deck:
+            mixed["memory_pressure_deck"] = memory_pressure_deck(local)
 
     # adjoint cost on the adjoint deck (32^3, 24 angles, 16 groups, nmom 2,
     # per-cell sigma_t +-10 %): one converged forward solve and one converged

@@ -70,7 +70,9 @@ typedef struct snap_ctx snap_ctx;
 int snap_create(const snap_config *cfg, int device, snap_ctx **out);
 int snap_destroy(snap_ctx *ctx);
 
-/* Bytes of device scratch the context holds. */
+/* Bytes of device scratch the context holds now (the per-octant flux slots
+ * are allocated on the first call that needs them: snap_sweep, the adjoint
+ * entry points; inner iterations and snap_transport_solve need none). */
 size_t snap_scratch_bytes(const snap_ctx *ctx);
 
 /* xs[g*C + c] = sig[g*nmat + mat[c]-1]

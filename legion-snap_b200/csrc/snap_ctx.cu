@@ -70,6 +70,7 @@ struct snap_ctx {
   double *d_old0 = nullptr;        // [G][C] scalar flux before the current inner sweep
   bool atomic_octants = true;      // inner iterations add octants straight into the flux
   void *d_slots = nullptr, *d_bx = nullptr, *d_by = nullptr;
+  size_t slots_bytes = 0;   // octant slots: allocated on first use (inner iterations need none)
   int *d_ctrl = nullptr;   // [n_items * TY progress][counter][error][violations]
   int *h_ctrl = nullptr;   // pinned: error, violations, largest change (float bits)
   float prev_inner_df = 0.0f;   // FP32 contexts: largest change of the previous inner iteration
@@ -280,6 +281,14 @@ int sweep_launches(snap_ctx *c, const void *qtot, const void *t_xs, cudaStream_t
   p.item_index = c->d_item_index;
   p.qtot = qtot;
   p.t_xs = t_xs;
+  if (!atomic_flux && !c->d_slots) {
+    if (cudaMalloc(&c->d_slots, c->slots_bytes) != cudaSuccess) {
+      cudaGetLastError();
+      c->d_slots = nullptr;
+      return fail(SNAP_ERR_OOM, "cannot allocate the octant flux slots");
+    }
+    c->scratch_bytes += c->slots_bytes;
+  }
   p.phi_slots = atomic_flux ? (void *)atomic_flux : c->d_slots;
   p.atomic_flux = atomic_flux ? 1 : 0;
   p.bx = c->d_bx;
@@ -504,7 +513,8 @@ int snap_create(const snap_config *cfg, int device, snap_ctx **out) {
   const size_t face_items = std::max((size_t)c->n_items, (size_t)2 * c->n_pair_items);
   const size_t bx_b = face_items * cfg->nz * c->shape.TY * c->AP * c->wsize;
   const size_t by_b = face_items * cfg->nz * 8 * c->AP * c->wsize;
-  if (cudaMalloc(&c->d_slots, slots_b) != cudaSuccess || cudaMalloc(&c->d_bx, bx_b) != cudaSuccess ||
+  c->slots_bytes = slots_b;
+  if (cudaMalloc(&c->d_bx, bx_b) != cudaSuccess ||
       cudaMalloc(&c->d_by, by_b) != cudaSuccess ||
       cudaMalloc((void **)&c->d_ctrl, sizeof(int) * (c->n_progress() + 4)) != cudaSuccess ||
       cudaMalloc((void **)&c->d_old0, sizeof(double) * (size_t)G * c->C) != cudaSuccess) {
@@ -512,7 +522,7 @@ int snap_create(const snap_config *cfg, int device, snap_ctx **out) {
     free_ctx(c);
     return fail(SNAP_ERR_OOM, "cannot allocate sweep scratch");
   }
-  c->scratch_bytes = slots_b + bx_b + by_b + sizeof(int) * (c->n_progress() + 4) +
+  c->scratch_bytes = bx_b + by_b + sizeof(int) * (c->n_progress() + 4) +
                      sizeof(double) * (size_t)G * c->C;
   if (const char *os = getenv("SNAP_B200_OCTANT_SLOTS")) c->atomic_octants = atoi(os) == 0;
   if (cudaMemset(c->d_ctrl, 0, sizeof(int) * (c->n_progress() + 4)) != cudaSuccess ||
@@ -729,7 +739,7 @@ int snap_transport_solve(snap_ctx *c, const int32_t *mat, const double *qi, cons
   if (cudaMalloc(&t_xs64, sizeof(double) * n) != cudaSuccess ||
       cudaMalloc(&s_xs, sizeof(double) * n * nmom) != cudaSuccess ||
       cudaMalloc(&q2grp, sizeof(double) * n * M) != cudaSuccess ||
-      cudaMalloc(&fpo, sizeof(double) * n * M) != cudaSuccess ||
+      cudaMalloc(&fpo, sizeof(double) * n) != cudaSuccess ||
       cudaMalloc(&qtot, c->wsize * n * M) != cudaSuccess) {
     cudaGetLastError();
     cleanup();
@@ -787,7 +797,7 @@ int snap_transport_solve(snap_ctx *c, const int32_t *mat, const double *qi, cons
         STEP(k_outer_source(qi, slgg, mat, flux, q2grp, G, c->cfg.nmat, nmom, M, C, st));
         ++c->launches;
       }
-      STEP(k_copy_moment0(flux, fpo, M, n, st));                   // save_fluxes -> flux0po
+      STEP(k_moment0(flux, fpo, M, n, st));                        // save_fluxes -> flux0po
       ++c->launches;
       bool inner_conv = false;
       int inners = 0;
@@ -806,7 +816,7 @@ int snap_transport_solve(snap_ctx *c, const int32_t *mat, const double *qi, cons
       if (lowp && far) {
         // FP64 outer residual: every scalar flux within kFar of the last outer?
         STEP(cudaMemsetAsync(c->violations(), 0, sizeof(int), st));
-        STEP(k_count_violations(flux, fpo, M, n, kFar, c->violations(), st));
+        STEP(k_test_change(flux, fpo, M, n, kFar, c->violations(), c->maxdf(), st));
         ++c->launches;
         int v = 0;
         rc = read_ctrl(c, st, &v);
@@ -816,7 +826,7 @@ int snap_transport_solve(snap_ctx *c, const int32_t *mat, const double *qi, cons
       // convergence only on an outer iteration with the FP64 source
       if (inner_conv && !use_tc) {
         STEP(cudaMemsetAsync(c->violations(), 0, sizeof(int), st));
-        STEP(k_count_violations(flux, fpo, M, n, 100.0 * info->epsi, c->violations(), st));
+        STEP(k_test_change(flux, fpo, M, n, 100.0 * info->epsi, c->violations(), c->maxdf(), st));
         ++c->launches;
         int v = 0;
         rc = read_ctrl(c, st, &v);
