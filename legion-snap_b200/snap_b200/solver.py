@@ -258,3 +258,37 @@ class Snap:
                    inners_per_outer=list(info.inners_per_outer[:info.outer_total]),
                    total_ms=info.total_ms, sweep_ms=info.sweep_ms, outers_lowp=info.outers_lowp)
         return flux, rec
+
+
+def fp64_finish(deck: Deck, dprob: dict, flux: torch.Tensor, outers: int = 1, device: int = 0):
+    """FP64 refinement of a mixed-precision solution: `outers` outer
+    iterations of the FP64 path (FP64 outer source, FP64 sweeps until the
+    inner test passes or iitm) started from `flux` (the converged FP32-form
+    flux moments, float64), through the task-level C ABI of an FP64 context.
+    The outer iteration contracts the FP32 rounding error like any other
+    error, so one outer removes most of it.  The FP32 context should be
+    destroyed first when memory is tight.  Returns the refined flux (a new
+    tensor) and the device time and iteration counts."""
+    snap = Snap(deck, precision="fp64", device=device)
+    try:
+        flux = flux.clone()
+        t_xs = snap.expand_cross_section(dprob["sigt"], dprob["mat"])
+        if "sigt_scale" in dprob:
+            t_xs *= dprob["sigt_scale"][None, :]
+        s_xs = snap.expand_scattering_cross_section(dprob["slgg"], dprob["mat"])
+        qtot = torch.empty_like(flux)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        inners = 0
+        for _ in range(outers):
+            q2 = snap.calc_outer_source(dprob["qi"], dprob["slgg"], dprob["mat"], flux)
+            for _ in range(deck.iitm):
+                inners += 1
+                if snap.inner_iteration(s_xs, q2, t_xs, flux, qtot):
+                    break
+        e1.record()
+        torch.cuda.synchronize()
+        return flux, dict(ms=e0.elapsed_time(e1), outers=outers, inner_iterations=inners)
+    finally:
+        snap.close()

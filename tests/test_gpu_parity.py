@@ -355,3 +355,24 @@ def test_fp32_solve_refines_lowp_source():
     assert rec["outers_lowp"] >= 1
     assert rec["outers_lowp"] < rec["outer_total"]
     assert rel_err(flux[..., 0].cpu().numpy(), ref[..., 0]) < FP32_TOL
+
+
+def test_fp64_finish_of_fp32_solve():
+    """One FP64 outer iteration started from the converged FP32-form flux
+    removes most of the FP32 rounding error (the refinement used for large
+    decks)."""
+    from snap_b200.solver import Snap, fp64_finish
+    d = P.Deck(16, 16, 16, nang=12, ng=6, nmom=2, epsi=1e-6, iitm=5, oitm=30)
+    prob = P.make_problem(d)
+    snap64 = Snap(d)
+    dp = snap64.device_problem(prob)
+    ref, _ = snap64.transport_solve(dp)
+    snap64.close()
+    snap32 = Snap(d, precision="fp32")
+    f32, _ = snap32.transport_solve(dp)
+    snap32.close()
+    fin, stats = fp64_finish(d, dp, f32)
+    e32 = rel_err(f32[..., 0].cpu().numpy(), ref[..., 0].cpu().numpy())
+    efin = rel_err(fin[..., 0].cpu().numpy(), ref[..., 0].cpu().numpy())
+    assert stats["inner_iterations"] >= 1
+    assert efin < max(2e-6, 0.5 * e32), (e32, efin)
