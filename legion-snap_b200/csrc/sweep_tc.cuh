@@ -93,7 +93,10 @@ struct Shape {
   static constexpr size_t SMEM_BYTES =
       sizeof(uint4) * (F1 + F2) + sizeof(float) * (NC * AP + YRING + PSI + XST + YST + ZR);
   // 168 registers at 3 CTAs per SM; 7 or more angle tiles need 255 (2 CTAs)
-  static constexpr int MIN_BLOCKS = NT >= 7 ? 2 : 3;
+#ifndef SNAP_SWEEP_TC32_BLOCKS
+#define SNAP_SWEEP_TC32_BLOCKS 3
+#endif
+  static constexpr int MIN_BLOCKS = NT >= 7 ? 2 : SNAP_SWEEP_TC32_BLOCKS;
 };
 
 template <int NT, int KT>
@@ -485,7 +488,8 @@ __global__ void __launch_bounds__(128, (Shape<NT, KT>::MIN_BLOCKS))
         if (lane == 0) {
           if (j + 1 < TY) st_release_cta(&s_full[j], s + 1);
           if (j > 0) st_release_cta(&s_used[j], s + 1);
-          if (prog_out && (((s - s_first) & 1) || s == s_last)) st_release_gpu(prog_out, s + 1);
+          if (prog_out && ((s - s_first + 1) % SNAP_SWEEP_PUBLISH_EVERY == 0 || s == s_last))
+            st_release_gpu(prog_out, s + 1);
         }
 
         // forward state for the adjoint (cell-average flux and fixup flags)
