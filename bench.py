@@ -301,6 +301,9 @@ def mixed_large_deck(local):
         res["solve_speedup_fp32_vs_fp64"] = res["fp64"]["solve_ms"] / res["fp32"]["solve_ms"]
     except Exception as e:   # report, do not lose the main bench line
         res["error"] = f"{type(e).__name__}: {e}"
+    # the library allocates with cudaMalloc: hand torch's cached blocks back
+    phi = None
+    torch.cuda.empty_cache()
     return res
 
 
@@ -320,6 +323,7 @@ def memory_pressure_deck(local):
            "units_per_sweep": d.units_per_sweep}
     old = os.environ.get("SNAP_B200_OCTANTS_PER_LAUNCH")
     os.environ["SNAP_B200_OCTANTS_PER_LAUNCH"] = "1"
+    torch.cuda.empty_cache()   # the library's own cudaMalloc needs the memory torch caches
     try:
         snap = Snap(d, precision="fp32", device=local)
         dp = snap.device_problem(P.make_problem(d))
