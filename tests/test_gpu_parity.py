@@ -376,3 +376,29 @@ def test_fp64_finish_of_fp32_solve():
     efin = rel_err(fin[..., 0].cpu().numpy(), ref[..., 0].cpu().numpy())
     assert stats["inner_iterations"] >= 1
     assert efin < max(2e-6, 0.5 * e32), (e32, efin)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_inner_iteration_atomic_octants_match_slots(prec, monkeypatch):
+    """Inner iterations add every octant straight into the flux; the
+    per-octant slots with a separate reduction (SNAP_B200_OCTANT_SLOTS=1) give
+    the same flux up to summation order, and the same inner test result."""
+    from snap_b200.solver import Snap
+    d = P.Deck(16, 16, 8, nang=12, ng=3, nmom=3)
+    prob = P.make_problem(d)
+    out = []
+    for slots in ("0", "1"):
+        monkeypatch.setenv("SNAP_B200_OCTANT_SLOTS", slots)
+        snap = Snap(d, precision=prec)
+        dp = snap.device_problem(prob)
+        t_xs = snap.expand_cross_section(dp["sigt"], dp["mat"]).to(snap.sweep_dtype).contiguous()
+        s_xs = snap.expand_scattering_cross_section(dp["slgg"], dp["mat"])
+        flux = dev(random_qtot(d, 3))
+        q2 = snap.calc_outer_source(dp["qi"], dp["slgg"], dp["mat"], flux)
+        qtot = torch.empty(d.ng, d.cells, d.cmom, dtype=snap.sweep_dtype, device="cuda")
+        convs = [snap.inner_iteration(s_xs, q2, t_xs, flux, qtot) for _ in range(2)]
+        out.append((flux.cpu().numpy(), convs))
+        snap.close()
+    tol = TOL if prec == "fp64" else 1e-6
+    assert moment_err(out[0][0], out[1][0]) < tol
+    assert out[0][1] == out[1][1]
