@@ -6,8 +6,40 @@
 #include "snap_oracle.h"
 
 #include <math.h>
+#include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
+
+static int g_threads = 1;
+void oracle_set_threads(int n) { g_threads = n < 1 ? 1 : (n > 256 ? 256 : n); }
+
+/* Runs body(arg, i) for i in [0, n) on g_threads POSIX threads (strided). */
+typedef struct {
+  void (*body)(void *, int);
+  void *arg;
+  int n, stride, first;
+} par_job;
+
+static void *par_worker(void *p) {
+  par_job *j = (par_job *)p;
+  for (int i = j->first; i < j->n; i += j->stride) j->body(j->arg, i);
+  return NULL;
+}
+
+static void par_for(int n, void (*body)(void *, int), void *arg) {
+  const int t = g_threads < n ? g_threads : n;
+  if (t <= 1) {
+    for (int i = 0; i < n; i++) body(arg, i);
+    return;
+  }
+  pthread_t th[256];
+  par_job jobs[256];
+  for (int k = 0; k < t; k++) {
+    jobs[k].body = body; jobs[k].arg = arg; jobs[k].n = n; jobs[k].stride = t; jobs[k].first = k;
+    pthread_create(&th[k], NULL, par_worker, &jobs[k]);
+  }
+  for (int k = 0; k < t; k++) pthread_join(th[k], NULL);
+}
 
 static inline int band_of(int k) {
   /* moment k of the 3-D expansion belongs to Legendre band l with
@@ -74,11 +106,22 @@ void oracle_expand_scattering(const oracle_geom *g, const double *slgg,
 /* outer.cc:107-217.  qo0 = qi + sum_{g2 != g1} slgg[g1][mat][g2][0]*flux0[g2]
  * (outer.cc:160-171); higher moments k use the Legendre order of their band
  * (outer.cc:196-207, generalised to all cmom-1 moments). */
-void oracle_outer_source(const oracle_geom *g, const double *qi, const double *slgg,
-                         const int32_t *mat, const double *flux, double *q2grp) {
+typedef struct {
+  const oracle_geom *g;
+  const double *qi, *slgg, *flux;
+  const int32_t *mat;
+  double *q2grp;
+} outer_args;
+
+static void outer_group(void *arg, int g1) {
+  const outer_args *x = (const outer_args *)arg;
+  const oracle_geom *g = x->g;
+  const double *qi = x->qi, *slgg = x->slgg, *flux = x->flux;
+  const int32_t *mat = x->mat;
+  double *q2grp = x->q2grp;
   const size_t C = (size_t)g->nx * g->ny * g->nz;
   const int ng = g->ng, nmat = g->nmat, nmom = g->nmom, cmom = g->cmom;
-  for (int g1 = 0; g1 < ng; g1++)
+  {
     for (size_t c = 0; c < C; c++) {
       const int m = mat[c] - 1;
       double q0 = qi[g1 * C + c];
@@ -99,6 +142,13 @@ void oracle_outer_source(const oracle_geom *g, const double *qi, const double *s
         q2grp[(g1 * C + c) * cmom + k] = qk;
       }
     }
+  }
+}
+
+void oracle_outer_source(const oracle_geom *g, const double *qi, const double *slgg,
+                         const int32_t *mat, const double *flux, double *q2grp) {
+  outer_args x = {g, qi, slgg, flux, mat, q2grp};
+  par_for(g->ng, outer_group, &x);
 }
 
 /* inner.cc:106-160: qtot[0] = q2grp0 + flux0*s_xs[0];
@@ -225,15 +275,26 @@ void oracle_sweep_octant_group(const oracle_geom *g, int corner, int group,
   free(buf);
 }
 
+typedef struct {
+  const oracle_geom *g;
+  const double *qtot, *t_xs;
+  double *flux;
+} sweep_args;
+
+static void sweep_group(void *arg, int grp) {
+  const sweep_args *x = (const sweep_args *)arg;
+  for (int corner = 0; corner < 8; corner++)
+    oracle_sweep_octant_group(x->g, corner, grp, x->qtot, x->t_xs, x->flux);
+}
+
 void oracle_sweep(const oracle_geom *g, const double *qtot, const double *t_xs,
                   double *flux) {
   const size_t C = (size_t)g->nx * g->ny * g->nz;
   /* snap.cc:494 zeroes flux0 before the sweeps; the restatement zeroes every
    * moment (the reference leaves fluxm stale, a bug for nmom > 1). */
   memset(flux, 0, sizeof(double) * C * g->ng * g->cmom);
-  for (int corner = 0; corner < 8; corner++)          /* snap.cc:865 */
-    for (int grp = 0; grp < g->ng; grp++)             /* snap.cc:872 */
-      oracle_sweep_octant_group(g, corner, grp, qtot, t_xs, flux);
+  sweep_args x = {g, qtot, t_xs, flux};
+  par_for(g->ng, sweep_group, &x);   /* groups: snap.cc:872; octants in order: :865 */
 }
 
 /* inner.cc:283-324 and outer.cc:354-403 (scalar moment only) */

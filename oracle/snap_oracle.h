@@ -68,9 +68,14 @@ void oracle_inner_source(const oracle_geom *g, const double *s_xs,
 void oracle_sweep_octant_group(const oracle_geom *g, int corner, int group,
                                const double *qtot, const double *t_xs,
                                double *flux);
-/* all 8 octants x all groups (flux zeroed first) */
+/* all 8 octants x all groups (flux zeroed first).  Groups are independent
+ * sweeps (snap.cc:865-887 launches one task per octant and group chunk); with
+ * oracle_set_threads(n > 1) they are spread over n POSIX threads, each group's
+ * octants still summed in octant order, so the result does not depend on n. */
 void oracle_sweep(const oracle_geom *g, const double *qtot, const double *t_xs,
                   double *flux);
+/* host threads used by oracle_sweep and oracle_outer_source (default 1) */
+void oracle_set_threads(int n);
 /* inner.cc:283-324 / outer.cc:354-403: returns 1 if converged */
 int oracle_test_convergence(const oracle_geom *g, const double *flux,
                             const double *flux_prev, double epsi);

@@ -14,7 +14,21 @@ saved as small .npz fixtures:
                   iteration record, per-group sums and maxima and 4096 seeded
                   sample entries of the converged scalar flux.
 
-Usage: python tests/golden/make_golden.py [deck1] [deck2p]
+The reference's CPU path cannot run nmom > 1 (its non-MMS sweep dereferences
+an unbound flux-moment accessor, sweep.cc:312-317 against :575-590), so the
+multi-moment benchmark decks are pinned by the oracle's C restatement
+(oracle/snap_oracle.c, itself checked against the reference build at nmom = 1
+and against deck1_ref/deck2p_ref above), run on all host threads:
+
+  deck2_oracle.npz  64^3, A=36, G=32, nmom=4 (deck 2 exactly, the benchmark
+                    configuration): iteration record, per-group sums and
+                    maxima of every moment, 4096 seeded samples of the
+                    converged scalar flux and 512 seeded samples of all 16
+                    moments.
+  deck4_oracle.npz  32^3, A=24, G=16, nmom=2 with the per-cell +-10 % sigma_t
+                    field (the adjoint deck's forward solve): the same items.
+
+Usage: python tests/golden/make_golden.py [deck1] [deck2p] [deck2] [deck4]
 """
 from __future__ import annotations
 
@@ -28,7 +42,7 @@ ROOT = pathlib.Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(ROOT / "legion-snap_b200"))
 
-from oracle.bindings import RefSnap, build  # noqa: E402
+from oracle.bindings import Oracle, RefSnap, build  # noqa: E402
 from snap_b200 import problem as P  # noqa: E402
 
 OUT = pathlib.Path(__file__).resolve().parent
@@ -65,6 +79,36 @@ def deck2p():
         inner_total=rec["inner_total"], outer_total=rec["outer_total"],
         converged=rec["converged"], inners_per_outer=np.array(rec["inners_per_outer"]),
         variant=rec["variant"], seconds=rec["seconds"], nthreads=rec["nthreads"])
+
+
+def oracle_fixture(name, d):
+    import os
+    prob = P.make_problem(d)
+    threads = os.cpu_count() or 1
+    t = time.time()
+    flux, rec = Oracle(d, threads=threads).solve(prob)
+    secs = time.time() - t
+    print(name, "oracle solve", secs, "s", rec)
+    rng = np.random.default_rng(2025)
+    gs = rng.integers(0, d.ng, 4096)
+    cs = rng.integers(0, d.cells, 4096)
+    mg = rng.integers(0, d.ng, 512)
+    mc = rng.integers(0, d.cells, 512)
+    np.savez_compressed(
+        OUT / f"{name}_oracle.npz", sample_g=gs, sample_c=cs, sample_flux0=flux[gs, cs, 0],
+        moment_g=mg, moment_c=mc, moment_flux=flux[mg, mc, :],
+        group_sum=flux.sum(axis=1), group_max=np.abs(flux).max(axis=1),
+        inner_total=rec["inner_total"], outer_total=rec["outer_total"],
+        converged=rec["converged"], inners_per_outer=np.array(rec["inners_per_outer"]),
+        seconds=secs, nthreads=threads)
+
+
+def deck2():
+    oracle_fixture("deck2", P.deck(2))
+
+
+def deck4():
+    oracle_fixture("deck4", P.deck(4))
 
 
 if __name__ == "__main__":

@@ -222,18 +222,52 @@ def test_solve_multimoment_matches_oracle():
     assert rec["inners_per_outer"] == rref["inners_per_outer"]
 
 
-def test_solve_deck2_full_size_properties():
-    """Deck 2 at full size (64^3, A=36, G=32, nmom=4): converges, stays finite
-    and positive, and keeps the problem's three mirror symmetries to 1e-12."""
+def check_oracle_fixture(g, flux, rec, tol):
+    """A converged solve against an oracle fixture (tests/golden/*_oracle.npz):
+    the scalar flux at the seeded samples, per-group sums and maxima (relative,
+    `tol`), every moment at the moment samples (`tol` of that moment's largest
+    magnitude), and the iteration record."""
+    f = flux.cpu().numpy()
+    phi = f[..., 0]
+    assert rel_err(phi[g["sample_g"], g["sample_c"]], g["sample_flux0"]) < tol
+    assert rel_err(f.sum(axis=1)[:, 0], g["group_sum"][:, 0]) < tol
+    assert rel_err(np.abs(f).max(axis=1)[:, 0], g["group_max"][:, 0]) < tol
+    scale = g["group_max"].max(axis=0)
+    mom = np.abs(f[g["moment_g"], g["moment_c"], :] - g["moment_flux"]).max(axis=0) / scale
+    assert float(mom.max()) < tol
+    assert rec["converged"] == bool(g["converged"])
+
+
+def test_solve_deck2_matches_oracle(golden_dir):
+    """Deck 2 exactly as benchmarked (64^3, A=36, G=32, nmom=4, 16 moments):
+    the oracle's converged solve at seeded samples, per-group sums and maxima,
+    all moments at seeded cells, the identical iteration record; and the
+    problem's three mirror symmetries to 1e-12."""
+    g = np.load(golden_dir / "deck2_oracle.npz")
     d = P.deck(2)
     snap = snap_ctx(d)
     flux, rec = snap.transport_solve(snap.device_problem(P.make_problem(d)))
-    assert rec["converged"]
+    check_oracle_fixture(g, flux, rec, TOL)
+    assert rec["inner_total"] == int(g["inner_total"])
+    assert rec["outer_total"] == int(g["outer_total"])
+    assert rec["inners_per_outer"] == list(g["inners_per_outer"])
     phi = flux[..., 0].reshape(d.ng, d.nz, d.ny, d.nx)
     assert torch.isfinite(flux).all()
     assert (phi > 0).all()
     for dim in (1, 2, 3):
         assert rel_err(phi.flip(dim).cpu().numpy(), phi.cpu().numpy()) < TOL
+
+
+def test_solve_deck4_matches_oracle(golden_dir):
+    """The adjoint deck's forward solve (32^3, A=24, G=16, nmom=2, per-cell
+    +-10 % sigma_t) against the oracle fixture at 1e-12, iteration record
+    identical."""
+    g = np.load(golden_dir / "deck4_oracle.npz")
+    d = P.deck(4)
+    snap = snap_ctx(d)
+    flux, rec = snap.transport_solve(snap.device_problem(P.make_problem(d)))
+    check_oracle_fixture(g, flux, rec, TOL)
+    assert rec["inners_per_outer"] == list(g["inners_per_outer"])
 
 
 # ---------------------------------------------------------------- FP32 form
@@ -243,6 +277,19 @@ FP32_TOL = 1e-5    # scalar-flux error of the FP32 form against the FP64 oracle
 def snap_ctx32(deck):
     from snap_b200.solver import Snap
     return Snap(deck, precision="fp32")
+
+
+def test_fp32_solve_deck2_error_against_oracle(golden_dir):
+    """The precision form's whole solve on deck 2 (FP32 sweep, BF16
+    tensor-core outer source while far from convergence, FP64 sources and
+    tests) against the FP64 oracle fixture: scalar flux within 1e-5 relative
+    at the samples and in the per-group sums and maxima, every moment within
+    1e-5 of its largest magnitude."""
+    g = np.load(golden_dir / "deck2_oracle.npz")
+    d = P.deck(2)
+    snap = snap_ctx32(d)
+    flux, rec = snap.transport_solve(snap.device_problem(P.make_problem(d)))
+    check_oracle_fixture(g, flux, rec, FP32_TOL)
 
 
 @pytest.mark.parametrize("d", [P.deck(1), P.Deck(16, 16, 16, nang=36, ng=3, nmom=4)],

@@ -129,3 +129,25 @@ def test_convergence_test_semantics():
     assert o.test_convergence(flux, prev, 1e-4)
     flux[0, 5, 0] = np.nan      # NaN compares false, counted as converged
     assert o.test_convergence(flux, prev, 1e-4)
+
+
+def test_oracle_threads_do_not_change_results():
+    """Groups spread over host threads: bitwise the same solve as one thread."""
+    d = P.Deck(8, 8, 8, nang=6, ng=5, nmom=2, epsi=1e-6, iitm=2, oitm=2)
+    prob = P.make_problem(d)
+    f1, r1 = Oracle(d, threads=1).solve(prob)
+    f4, r4 = Oracle(d, threads=4).solve(prob)
+    assert np.array_equal(f1, f4)
+    assert r1 == r4
+
+
+def test_oracle_reproduces_deck4_fixture(golden_dir):
+    """The committed adjoint-deck fixture (tests/golden/deck4_oracle.npz)
+    is what the oracle computes (the GPU tests compare against it)."""
+    import os
+    g = np.load(golden_dir / "deck4_oracle.npz")
+    d = P.deck(4)
+    f, rec = Oracle(d, threads=os.cpu_count() or 1).solve(P.make_problem(d))
+    assert np.array_equal(f[g["sample_g"], g["sample_c"], 0], g["sample_flux0"])
+    assert np.array_equal(f[g["moment_g"], g["moment_c"], :], g["moment_flux"])
+    assert rec["inners_per_outer"] == list(g["inners_per_outer"])
