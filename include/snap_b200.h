@@ -64,7 +64,10 @@ typedef struct snap_ctx snap_ctx;
 
 /* Creates a context on `device`: uploads the quadrature, builds the per-octant
  * coefficient tables and allocates the sweep's scratch (per-octant flux
- * slots, tile-boundary faces, progress flags).
+ * slots, tile-boundary faces, progress flags).  Shapes outside the tiled
+ * sweep kernel (nx not a multiple of 8, ny not a multiple of 4, more than 64
+ * angles per octant) run every forward sweep on the general kernel (one CTA
+ * per octant and group, up to 2048 angles; FP64 contexts only; no adjoint).
  * Replaces InitGPUSweep -> initialize_gpu_context (init.cc:215-236,
  * gpu_sweep.cu:71-273). */
 int snap_create(const snap_config *cfg, int device, snap_ctx **out);
@@ -168,6 +171,14 @@ typedef struct {
 /* Accumulated timing of this context since creation or the last reset. */
 int snap_get_timing(snap_ctx *ctx, snap_timing *out, int reset);
 
+/* One line of the reference's convergence log (convergence.cc:154-232). */
+typedef struct {
+  int kind;            /* 0: an inner iteration and its inner test, 1: an outer test */
+  int time_step, outer, inner;   /* 0-based numbers, as the reference prints them */
+  int converged;
+  double us;           /* host wall time: the inner iteration, or the whole outer iteration */
+} snap_iter_record;
+
 typedef struct {
   double epsi;
   int iitm, oitm;
@@ -177,6 +188,10 @@ typedef struct {
   double sweep_ms;     /* device time spent in the sweep kernels */
   double total_ms;     /* device time of the whole solve */
   int outers_lowp;     /* outer iterations whose source came from the BF16 tensor cores */
+  /* optional HOST array for the iteration log: records_cap entries, NULL
+   * for none; records_len reports how many were written */
+  snap_iter_record *records;
+  int records_cap, records_len;
 } snap_solve_info;
 
 /* Full steady-state fixed-source solve, the sequential semantics of the
@@ -194,6 +209,69 @@ typedef struct {
 int snap_transport_solve(snap_ctx *ctx, const int32_t *mat, const double *qi,
                          const double *sigt, const double *slgg, const double *sigt_scale,
                          double *flux, snap_solve_info *info, void *stream);
+
+/* Time stepping of a time-dependent solve (the reference's timedep = 1
+ * decks: input/*_1x1x1.in, input/mms.in). */
+typedef struct {
+  int nsteps;            /* time steps (the time loop of snap.cc:409-541) */
+  double dt;             /* time-step length, tf / nsteps (snap.cc:1174) */
+  const double *vdelt;   /* DEVICE [ng]: 2 / (dt v_g); NULL: the reference's
+                            speeds v_g = ng - g (snap.cc:717-739) */
+  double *psi_t;         /* DEVICE scratch of 2 * 8 * ng * C * nang doubles: the
+                            angular flux at the two edges of a time step, laid
+                            out [2][octant][g][c][angle] (the reference's
+                            time_flux_even / time_flux_odd, snap.cc:288-298);
+                            NULL: allocated and freed by the call */
+  int psi_t_initialised; /* 0: psi_t is zeroed first (snap.cc:341-344);
+                            1: its first half holds the initial angular flux */
+  double *qim;           /* DEVICE [octant][g][c][angle] per-angle source added
+                            to the angular source (the MMS source,
+                            sweep.cc:368-375), or NULL */
+  int qim_time_scaled;   /* 1: qim is multiplied in place at the start of
+                            every time step by the reference's MMS factors
+                            (dt/2, then (2cy+1)/(2cy-1); snap.cc:451-466) */
+} snap_time_config;
+
+/* Time-dependent solve: tc->nsteps time steps of the steady-state loop of
+ * snap_transport_solve (outer source, inner source, sweep, inner and outer
+ * tests per step; the flux carries over between steps), with the
+ * time-dependent sweep: vdelt * psi_t_in added to the diamond-difference
+ * numerator and vdelt to its denominator, psi_t_out = 2 pc - psi_t_in as a
+ * fourth outgoing face (with its own fixup flag), the two halves of psi_t
+ * swapping roles every step.  Replaces Snap::transport_solve with
+ * time_dependent = true (snap.cc:409-541, sweep.cc:413-419, 461-468, 473-518).
+ * The sweep is the general kernel (any mesh, up to 2048 angles per octant).
+ * FP64 contexts.  info->inners_per_outer lists the outer iterations of all
+ * steps in order. */
+int snap_transport_solve_td(snap_ctx *ctx, const int32_t *mat, const double *qi,
+                            const double *sigt, const double *slgg, const double *sigt_scale,
+                            const snap_time_config *tc, double *flux, snap_solve_info *info,
+                            void *stream);
+
+/* ---- Manufactured-solution check (the reference's src_opt = 3 decks) ---- */
+
+/* The manufactured solution of the reference's MMS check for the context's
+ * mesh (nmom = 1): ref_flux [G][C] = (g+1) X(x) Y(y) Z(z), the cell averages
+ * of sin(pi x/lx) sin(pi y/ly) sin(pi z/lz) (mms.cc:83-179), and the per-angle
+ * source qim [8][G][C][nang] that makes it the solution: its streaming term
+ * in each octant's direction, the removal sigt * ref, minus the scattering
+ * of every group into g (mms.cc:211-359).  timedep != 0: qi [G][C] =
+ * ref_flux / v_g and ref_flux scaled to tf - dt/2, the solution at the middle
+ * of the last step (mms.cc:387-418); then pass qim to snap_transport_solve_td
+ * with qim_time_scaled = 1.  sigt [G][nmat] and slgg as for the solve.
+ * Replaces MMSInitFlux, MMSInitSource and MMSInitTimeDependent
+ * (snap.cc:373-388).  Synchronises `stream`. */
+int snap_mms_init(snap_ctx *ctx, const int32_t *mat, const double *sigt, const double *slgg,
+                  double lx, double ly, double lz, int timedep, double tf, double dt,
+                  double *ref_flux, double *qim, double *qi, void *stream);
+
+/* out[0], out[1], out[2] = max, min and sum over cells and groups of
+ * |flux/ref - 1| (|flux| where ref < 1e-12); flux holds cmom moments per
+ * cell (the scalar one is compared).  The reference fails the check when the
+ * max exceeds 0.1 or the sum / (cells * groups) exceeds 1e-3 (snap.cc:542-560).
+ * Replaces MMSCompare (mms.cc:498-545).  Synchronises `stream`. */
+int snap_mms_compare(snap_ctx *ctx, const double *flux, const double *ref_flux, double *out,
+                     void *stream);
 
 /* ---- Sensitivities (no counterpart in the reference) ------------------ */
 
@@ -243,13 +321,18 @@ int snap_adjoint_solve(snap_ctx *ctx, const int32_t *mat, const double *qi, cons
  * Takes the configuration directly (cfg->precision must be SNAP_FP64; host
  * quadrature arrays as for snap_create) and device qtot, t_xs and flux
  * arrays as snap_sweep does.  It allocates nothing: its scratch is one
- * static device array of SNAP_NOALLOC_SCRATCH_BYTES bytes that every GPU
- * loading this library holds until exit, and problems needing more return
- * SNAP_ERR_UNSUPPORTED with the size in snap_last_error().  Every call
- * shares that array (it keeps the last call's contents; each call clears
- * what must start at zero), so calls that overlap on the GPU race.  The
- * first call on a device looks the array's device address up; make it before
- * any stream capture on that device.  Synchronises `stream`.
+ * static device array of SNAP_NOALLOC_SCRATCH_BYTES bytes, and problems
+ * needing more return SNAP_ERR_UNSUPPORTED with the size in
+ * snap_last_error().  CUDA loads code lazily, so the array and the sweep's
+ * code are placed on a device when first used there and held until the
+ * process exits: call once with qtot, t_xs and flux all NULL (set-up only:
+ * nothing is launched), with the device current, outside any section that
+ * must not allocate; otherwise the first sweep does this.  Every call shares
+ * that array (it keeps the last call's contents; each call clears what must
+ * start at zero), so calls that overlap on the GPU race.  The first call on
+ * a device looks the array's device address up and keeps it; make it before
+ * any stream capture on that device, and make no call after a
+ * cudaDeviceReset of it.  Synchronises `stream` (except the set-up call).
  * No counterpart in the reference. */
 int snap_sweep_noalloc(const snap_config *cfg, const double *qtot, const double *t_xs,
                        double *flux, void *stream);
@@ -264,6 +347,15 @@ int snap_sweep_noalloc(const snap_config *cfg, const double *qtot, const double 
  * out[4i+3] = the correctly rounded a[i]/b[i].  Does not synchronise. */
 int snap_selftest_division(int precision, const void *a, const void *b, long long n, void *out,
                            void *stream);
+
+/* Fault injection for tests of the bounded device-side waits (no
+ * counterpart in the reference): in the next sweep launch of this context,
+ * the warps of work item `item` (0 .. items per launch - 1; item 0 is the
+ * first tile of the first octant and group) never publish their tile-edge
+ * progress, so the tiles downstream of it wait until their limit
+ * (SNAP_B200_TIMEOUT_MS, read at snap_create), give up, and the call returns
+ * SNAP_ERR_DEVICE_TIMEOUT.  One launch only; the context stays usable. */
+int snap_inject_stall(snap_ctx *ctx, int item);
 
 /* Last error message of this thread (static storage). */
 const char *snap_last_error(void);

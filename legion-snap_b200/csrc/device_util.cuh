@@ -8,8 +8,10 @@ namespace snapb200 {
 
 // D(8x8) += A(8x4, row) * B(4x8, col) in FP64 on the tensor cores.
 // Lane l holds A[l/4][l%4], B[l%4][l/4] and D[l/4][2(l%4)+{0,1}].
+// Not volatile: the MMA has no side effects, so the compiler may interleave
+// independent accumulator chains instead of issuing them in source order.
 __device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a, double b) {
-  asm volatile(
+  asm(
       "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
       : "+d"(c0), "+d"(c1)
       : "d"(a), "d"(b));

@@ -23,6 +23,7 @@ struct SweepParams {
   int accumulate;  // add into the flux slots instead of storing
   int atomic_flux; // phi_slots is the FP64 flux [G][C][M]: every octant adds into it atomically
   int fixup;
+  int withhold_item1;     // fault injection: work item + 1 whose warps never publish progress (0: none)
   long long timeout_ns;
   const int *item_table;  // item -> (sweep << 16) | (tx << 8) | ty
   const int *item_index;  // [sweep][tx][ty] -> item
@@ -46,6 +47,50 @@ struct SweepParams {
   // Adjoint sweep only: the adjoint of t_xs per octant slot, [P][G][C].
   void *sigt_bar_slots;
 };
+
+// Parameters of the general sweep (sweep_wide.cu): one CTA per (octant,
+// group), threads over angles, cells one at a time.  FP64 throughout.
+struct WideParams {
+  int nx, ny, nz;
+  int A;            // angles per octant
+  int M;            // flux moments (cmom)
+  int G;            // groups
+  int o_base;       // first octant of this launch (the grid covers octants o_base.. x G)
+  int fixup;
+  int td;           // time dependent: vdelt, tf_in and tf_out are used
+  double hi, hj, hk;
+  const double *mu, *eta, *xi, *w;   // [A]
+  const double *ec;                  // [8][M][A]
+  const double *qtot;                // [G][C][M]
+  const double *t_xs;                // [G][C]
+  const double *vdelt;               // [G]
+  const double *tf_in;               // [8][G][C][A] angular flux at the start of the time step
+  double *tf_out;                    // [8][G][C][A] angular flux at its end
+  const double *qim;                 // [8][G][C][A] manufactured per-angle source, or null
+  double *flux;                      // [G][C][M], every octant added atomically
+  double *ypen;                      // scratch [blocks][nx][A]
+  double *zpl;                       // scratch [blocks][ny*nx][A]
+};
+int wide_threads(int A);
+size_t wide_smem_bytes(int A, int nx, int M);
+bool wide_supported(int A, int nx, int M);
+cudaError_t launch_sweep_wide(const WideParams &p, int n_blocks, cudaStream_t st);
+
+// The manufactured-solution check (mms.cu).
+struct MmsGeometry {
+  int nx, ny, nz, A, G, nmat;
+  double lx, ly, lz;
+  int timedep;
+  double tf, dt;
+  const double *quad[3];   // host mu, eta, xi [A]
+};
+size_t mms_scratch_words(int nx, int ny, int nz, int A);
+cudaError_t mms_init(const MmsGeometry &geo, const int32_t *mat, const double *sigt,
+                     const double *slgg, double *ref, double *qim, double *qi, double *scratch,
+                     cudaStream_t st);
+// out = {max, min, sum} of |flux/ref - 1|; scratch: 3 words of device memory
+cudaError_t mms_compare(const double *flux, int M, const double *ref, long long n, void *scratch,
+                        double out[3], cudaStream_t st);
 
 // Per-precision static configuration picked at context creation.
 struct SweepShape {
@@ -129,6 +174,8 @@ cudaError_t k_reduce_slots(const void *slots, int nslots, int fp32, void *flux_o
 cudaError_t k_count_violations(const double *flux, const double *prev, int M, long long n,
                                double epsi, int *violations, cudaStream_t st);
 cudaError_t k_to_f32(const double *in, float *out, long long n, cudaStream_t st);
+// x[i] *= f
+cudaError_t k_scale(double *x, double f, size_t n, cudaStream_t st);
 // phi_bar[g'][c][k] = r[g'][c] (k = 0) + sum_g slgg[g][mat][g'][l(k)] qbar[g][c][k]
 cudaError_t k_adjoint_scatter(const double *r, const double *slgg, const int32_t *mat,
                               const double *qbar, double *phi_bar, int G, int nmat, int nmom,

@@ -288,6 +288,13 @@ __global__ void max_abs_diff_kernel(const double *__restrict__ a, const double *
   }
 }
 
+// mms.cc:442-470 (MMSScale): x *= f
+__global__ void scale_kernel(double *__restrict__ x, double f, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    x[i] *= f;
+}
+
 __global__ void to_f32_kernel(const double *__restrict__ in, float *__restrict__ out, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
@@ -330,6 +337,11 @@ cudaError_t k_max_abs_diff(const double *a, const double *b, long long n,
 
 cudaError_t k_to_f32(const double *in, float *out, long long n, cudaStream_t st) {
   to_f32_kernel<<<grid_for(n), BLK, 0, st>>>(in, out, n);
+  return cudaGetLastError();
+}
+
+cudaError_t k_scale(double *x, double f, size_t n, cudaStream_t st) {
+  scale_kernel<<<grid_for((long long)n), BLK, 0, st>>>(x, f, (long long)n);
   return cudaGetLastError();
 }
 

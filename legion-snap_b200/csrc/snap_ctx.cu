@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -74,6 +75,19 @@ struct snap_ctx {
   int *d_ctrl = nullptr;   // [n_items * TY progress][counter][error][violations]
   int *h_ctrl = nullptr;   // pinned: error, violations, largest change (float bits)
   float prev_inner_df = 0.0f;   // FP32 contexts: largest change of the previous inner iteration
+  int withhold_item1 = 0;       // snap_inject_stall: work item + 1 of the next sweep launch
+  // general sweep (sweep_wide.cu): shapes the tiled kernel does not cover
+  // (ragged meshes, more than 64 angles) and every time-dependent sweep
+  bool wide_only = false;       // the tiled kernel cannot run this shape
+  double *d_wquad = nullptr;    // [mu, eta, xi, w: 4*A][ec: 8*M*A]
+  double *d_wscratch = nullptr; // y pencils and z planes of 8*G blocks
+  double *d_vdelt0 = nullptr;   // [G] zeros: steady-state vdelt
+  double *d_vdelt = nullptr;    // [G] vdelt of the current time-dependent solve
+  std::vector<double> h_vdelt;
+  // solve arrays, kept between snap_transport_solve calls (first call allocates)
+  void *d_solve = nullptr;
+  double *s_txs64 = nullptr, *s_sxs = nullptr, *s_q2 = nullptr, *s_fpo = nullptr;
+  void *s_qtot = nullptr, *s_txsw = nullptr;
   size_t scratch_bytes = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;   // whole-solve timing
   cudaEvent_t sw0 = nullptr, sw1 = nullptr;   // sweep timing
@@ -112,6 +126,11 @@ void free_ctx(snap_ctx *c) {
   cudaFree(c->d_bx);
   cudaFree(c->d_by);
   cudaFree(c->d_ctrl);
+  cudaFree(c->d_wquad);
+  cudaFree(c->d_wscratch);
+  cudaFree(c->d_vdelt0);
+  cudaFree(c->d_vdelt);
+  cudaFree(c->d_solve);
   if (c->h_ctrl) cudaFreeHost(c->h_ctrl);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
@@ -277,6 +296,8 @@ int sweep_launches(snap_ctx *c, const void *qtot, const void *t_xs, cudaStream_t
   p.n_items = c->n_items;
   p.fixup = c->cfg.fixup;
   p.timeout_ns = c->timeout_ns;
+  p.withhold_item1 = mode == 2 ? 0 : c->withhold_item1;
+  c->withhold_item1 = 0;   // one launch only
   p.item_table = c->d_item_table;
   p.item_index = c->d_item_index;
   p.qtot = qtot;
@@ -372,6 +393,92 @@ int read_ctrl(snap_ctx *c, cudaStream_t st, int *violations) {
   return SNAP_OK;
 }
 
+// Time-dependent terms of one inner iteration's sweep.
+struct TdArgs {
+  const double *vdelt;   // [G]
+  const double *tf_in;   // [8][G][C][A]
+  double *tf_out;        // [8][G][C][A]
+  const double *qim;     // [8][G][C][A] or null
+};
+int inner_iteration_impl(snap_ctx *c, const double *s_xs, const double *q2grp, const void *t_xs,
+                         double *flux, void *qtot, double epsi, int *converged, cudaStream_t st,
+                         const TdArgs *td);
+int solve_impl(snap_ctx *c, const int32_t *mat, const double *qi, const double *sigt,
+               const double *slgg, const double *sigt_scale, double *flux, snap_solve_info *info,
+               cudaStream_t st, const snap_time_config *tc);
+
+// Device quadrature tables and face scratch of the general sweep (allocated
+// on first use).
+int ensure_wide(snap_ctx *c) {
+  if (c->d_wscratch) return SNAP_OK;
+  const int A = c->A, M = c->M, G = c->cfg.ng;
+  if (!wide_supported(A, c->cfg.nx, M))
+    return fail(SNAP_ERR_UNSUPPORTED, "no general sweep for this shape");
+  std::vector<double> q((size_t)4 * A + (size_t)8 * M * A);
+  for (int a = 0; a < A; ++a) {
+    q[a] = c->mu[a];
+    q[A + a] = c->eta[a];
+    q[2 * A + a] = c->xi[a];
+    q[3 * A + a] = c->w[a];
+  }
+  std::copy(c->ec.begin(), c->ec.end(), q.begin() + 4 * A);
+  int rc = upload((void **)&c->d_wquad, q);
+  if (rc) return rc;
+  const size_t per_block = (size_t)c->cfg.nx * (1 + c->cfg.ny) * A;
+  const size_t bytes = sizeof(double) * per_block * 8 * G;
+  if (cudaMalloc((void **)&c->d_wscratch, bytes) != cudaSuccess ||
+      cudaMalloc((void **)&c->d_vdelt0, sizeof(double) * G) != cudaSuccess ||
+      cudaMemset(c->d_vdelt0, 0, sizeof(double) * G) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(c->d_wscratch);
+    c->d_wscratch = nullptr;
+    return fail(SNAP_ERR_OOM, "cannot allocate the general sweep's face scratch");
+  }
+  c->scratch_bytes += bytes + sizeof(double) * G;
+  return SNAP_OK;
+}
+
+// One general sweep of all 8 octants and groups, adding every octant's
+// moments into `flux` (double).  td != 0: time-dependent terms with vdelt
+// [G], tf_in/tf_out [8][G][C][A]; qim: per-angle source or null.
+int wide_sweep(snap_ctx *c, const double *qtot, const double *t_xs, double *flux,
+               const double *vdelt, const double *tf_in, double *tf_out, const double *qim,
+               cudaStream_t st) {
+  int rc = ensure_wide(c);
+  if (rc) return rc;
+  const int A = c->A, M = c->M, G = c->cfg.ng;
+  WideParams p{};
+  p.nx = c->cfg.nx;
+  p.ny = c->cfg.ny;
+  p.nz = c->cfg.nz;
+  p.A = A;
+  p.M = M;
+  p.G = G;
+  p.o_base = 0;
+  p.fixup = c->cfg.fixup;
+  p.td = (vdelt && tf_in && tf_out) ? 1 : 0;
+  p.hi = c->cfg.hi;
+  p.hj = c->cfg.hj;
+  p.hk = c->cfg.hk;
+  p.mu = c->d_wquad;
+  p.eta = c->d_wquad + A;
+  p.xi = c->d_wquad + 2 * A;
+  p.w = c->d_wquad + 3 * A;
+  p.ec = c->d_wquad + 4 * A;
+  p.qtot = qtot;
+  p.t_xs = t_xs;
+  p.vdelt = p.td ? vdelt : c->d_vdelt0;
+  p.tf_in = tf_in;
+  p.tf_out = tf_out;
+  p.qim = qim;
+  p.flux = flux;
+  p.ypen = c->d_wscratch;
+  p.zpl = c->d_wscratch + (size_t)c->cfg.nx * A * 8 * G;
+  SNAP_CUDA(launch_sweep_wide(p, 8 * G, st));
+  ++c->launches;
+  return SNAP_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -388,12 +495,19 @@ int snap_create(const snap_config *cfg, int device, snap_ctx **out) {
     return fail(SNAP_ERR_BAD_ARG, "unknown precision");
   int tile_y = cfg->ny % 4 == 0 ? 4 : 8;
   if (const char *te = getenv("SNAP_B200_TILE_Y")) tile_y = atoi(te) == 8 ? 8 : 4;
-  if (cfg->nx % 8 || cfg->ny % tile_y)
-    return fail(SNAP_ERR_UNSUPPORTED, "nx must be a multiple of 8 and ny of the tile height");
-  if (cfg->nang > 64) return fail(SNAP_ERR_UNSUPPORTED, "at most 64 angles per octant");
-  if (cfg->nx / 8 > 255 || cfg->ny / 8 > 255)
-    return fail(SNAP_ERR_UNSUPPORTED, "at most 2040 cells along x and y");
-  if ((long long)8 * cfg->ng >= 32768) return fail(SNAP_ERR_UNSUPPORTED, "too many groups");
+  // the tiled kernel: 8 x tile_y column tiles, at most 64 angles in registers;
+  // other shapes run the general sweep (FP64 only, forward sweeps only)
+  const bool tiled_ok = cfg->nx % 8 == 0 && cfg->ny % tile_y == 0 && cfg->nang <= 64 &&
+                        cfg->nx / 8 <= 255 && cfg->ny / 8 <= 255 &&
+                        (long long)8 * cfg->ng < 32768 &&
+                        (long long)cfg->nx * cfg->ny * cfg->nz * cfg->nmom * cfg->nmom < (1LL << 31);
+  if (!tiled_ok) {
+    if (cfg->precision != SNAP_FP64)
+      return fail(SNAP_ERR_UNSUPPORTED,
+                  "FP32 sweeps need nx % 8 == 0, ny % 4 == 0 and at most 64 angles per octant");
+    if (!wide_supported(cfg->nang, cfg->nx, cfg->nmom * cfg->nmom))
+      return fail(SNAP_ERR_UNSUPPORTED, "at most 2048 angles per octant");
+  }
 
   snap_ctx *c = new snap_ctx();
   c->cfg = *cfg;
@@ -422,9 +536,38 @@ int snap_create(const snap_config *cfg, int device, snap_ctx **out) {
   c->AP = 8 * c->shape.NT;
   c->wsize = c->fp32 ? sizeof(float) : sizeof(double);
   const bool ok = c->fp32 ? sweep_fp32_supported(c->shape) : sweep_fp64_supported(c->shape);
-  if (!ok) {
-    free_ctx(c);
-    return fail(SNAP_ERR_UNSUPPORTED, "no compiled sweep kernel for this shape");
+  if (!tiled_ok || !ok) {
+    if (c->fp32 || !wide_supported(c->A, cfg->nx, c->M)) {
+      free_ctx(c);
+      return fail(SNAP_ERR_UNSUPPORTED, "no compiled sweep kernel for this shape");
+    }
+    // general sweep only: no tiled tables or tile scratch
+    c->wide_only = true;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+      free_ctx(c);
+      return cuda_fail(e, "cudaSetDevice");
+    }
+    c->P = 8;
+    c->n_items = 0;
+    if (cudaMalloc((void **)&c->d_ctrl, sizeof(int) * 4) != cudaSuccess ||
+        cudaMalloc((void **)&c->d_old0, sizeof(double) * (size_t)cfg->ng * c->C) != cudaSuccess ||
+        cudaMemset(c->d_ctrl, 0, sizeof(int) * 4) != cudaSuccess ||
+        cudaMallocHost((void **)&c->h_ctrl, 4 * sizeof(int)) != cudaSuccess ||
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+        cudaEventCreate(&c->sw0) != cudaSuccess || cudaEventCreate(&c->sw1) != cudaSuccess) {
+      cudaGetLastError();
+      free_ctx(c);
+      return fail(SNAP_ERR_OOM, "cannot allocate context buffers");
+    }
+    c->scratch_bytes = sizeof(int) * 4 + sizeof(double) * (size_t)cfg->ng * c->C;
+    int rc = ensure_wide(c);
+    if (rc) {
+      free_ctx(c);
+      return rc;
+    }
+    *out = c;
+    return SNAP_OK;
   }
   c->tiles_x = cfg->nx / 8;
   c->tiles_y = cfg->ny / c->shape.TY;
@@ -562,6 +705,15 @@ int snap_destroy(snap_ctx *ctx) {
 
 size_t snap_scratch_bytes(const snap_ctx *ctx) { return ctx ? ctx->scratch_bytes : 0; }
 
+int snap_inject_stall(snap_ctx *c, int item) {
+  if (!c) return fail(SNAP_ERR_BAD_ARG, "null context");
+  if (c->tc32 || c->wide_only)
+    return fail(SNAP_ERR_UNSUPPORTED, "not available with the TF32 or the general sweep kernel");
+  if (item < 0 || item >= c->n_items) return fail(SNAP_ERR_BAD_ARG, "work item out of range");
+  c->withhold_item1 = item + 1;
+  return SNAP_OK;
+}
+
 int snap_expand_xs(snap_ctx *c, const double *sig, const int32_t *mat, double *xs, void *stream) {
   if (!c || !sig || !mat || !xs) return fail(SNAP_ERR_BAD_ARG, "null argument");
   SNAP_CUDA(k_expand_xs(sig, mat, xs, c->cfg.ng, c->cfg.nmat, c->C, (cudaStream_t)stream));
@@ -631,6 +783,17 @@ int snap_sweep(snap_ctx *c, const void *qtot, const void *t_xs, void *flux, void
   if (!c || !qtot || !t_xs || !flux) return fail(SNAP_ERR_BAD_ARG, "null argument");
   cudaStream_t st = (cudaStream_t)stream;
   SNAP_CUDA(cudaMemsetAsync(c->error(), 0, 2 * sizeof(int), st));
+  if (c->wide_only) {
+    SNAP_CUDA(cudaMemsetAsync(flux, 0, sizeof(double) * c->cfg.ng * c->C * c->M, st));
+    SNAP_CUDA(cudaEventRecord(c->sw0, st));
+    int rc = wide_sweep(c, (const double *)qtot, (const double *)t_xs, (double *)flux, nullptr,
+                        nullptr, nullptr, nullptr, st);
+    if (rc) return rc;
+    SNAP_CUDA(cudaEventRecord(c->sw1, st));
+    rc = read_ctrl(c, st, nullptr);
+    if (rc == SNAP_OK) account_sweep(c);
+    return rc;
+  }
   int rc = timed_sweep(c, qtot, t_xs, flux, c->fp32, nullptr, 0, 0.0, st);
   if (rc) return rc;
   rc = read_ctrl(c, st, nullptr);
@@ -642,7 +805,20 @@ int snap_inner_iteration(snap_ctx *c, const double *s_xs, const double *q2grp, c
                          double *flux, void *qtot, double epsi, int *converged, void *stream) {
   if (!c || !s_xs || !q2grp || !t_xs || !flux || !qtot || !converged)
     return fail(SNAP_ERR_BAD_ARG, "null argument");
-  cudaStream_t st = (cudaStream_t)stream;
+  return inner_iteration_impl(c, s_xs, q2grp, t_xs, flux, qtot, epsi, converged,
+                              (cudaStream_t)stream, nullptr);
+}
+
+}  // extern "C"
+
+namespace {
+
+// The inner-loop body (snap.cc:487-503).  td != null: the time-dependent
+// sweep of the general kernel (vdelt, the time-edge angular flux, the
+// manufactured source).
+int inner_iteration_impl(snap_ctx *c, const double *s_xs, const double *q2grp, const void *t_xs,
+                         double *flux, void *qtot, double epsi, int *converged, cudaStream_t st,
+                         const TdArgs *td) {
   SNAP_CUDA(cudaMemsetAsync(c->error(), 0, 3 * sizeof(int), st));
   // FP32 contexts: the sweep's rounding leaves a per-inner change of about
   // 1e-6 (max over cells) that no iteration removes, so the inner test
@@ -650,7 +826,19 @@ int snap_inner_iteration(snap_ctx *c, const double *s_xs, const double *q2grp, c
   constexpr double kFp32InnerFloor = 32.0 / 16777216.0;
   const double eps_in = c->fp32 ? std::max(epsi, kFp32InnerFloor) : epsi;
   int rc = SNAP_OK;
-  if (c->atomic_octants && !c->tc32) {
+  if (c->wide_only || td) {
+    SNAP_CUDA(k_inner_source_save(s_xs, q2grp, flux, qtot, 0, c->d_old0, c->cfg.ng, c->cfg.nmom,
+                                  c->M, c->C, st));
+    SNAP_CUDA(cudaEventRecord(c->sw0, st));
+    rc = wide_sweep(c, (const double *)qtot, (const double *)t_xs, flux,
+                    td ? td->vdelt : nullptr, td ? td->tf_in : nullptr,
+                    td ? td->tf_out : nullptr, td ? td->qim : nullptr, st);
+    if (rc) return rc;
+    SNAP_CUDA(cudaEventRecord(c->sw1, st));
+    SNAP_CUDA(k_test_change(flux, c->d_old0, c->M, (long long)c->cfg.ng * c->C, eps_in,
+                            c->violations(), c->maxdf(), st));
+    c->launches += 2;
+  } else if (c->atomic_octants && !c->tc32) {
     // inner source, old scalar flux saved and flux cleared in one pass; the
     // sweep adds every octant into the flux; the inner test reads it back
     SNAP_CUDA(k_inner_source_save(s_xs, q2grp, flux, qtot, c->fp32, c->d_old0, c->cfg.ng,
@@ -687,6 +875,277 @@ int snap_inner_iteration(snap_ctx *c, const double *s_xs, const double *q2grp, c
   return SNAP_OK;
 }
 
+// Solve arrays kept by the context between solves (allocated on the first).
+int ensure_solve_arrays(snap_ctx *c) {
+  if (c->d_solve) return SNAP_OK;
+  const long long n = (long long)c->cfg.ng * c->C;
+  const size_t t64 = sizeof(double) * n, sxs = sizeof(double) * n * c->cfg.nmom,
+               q2 = sizeof(double) * n * c->M, fpo = sizeof(double) * n,
+               qt = c->wsize * n * c->M, tsw = c->fp32 ? sizeof(float) * n : 0;
+  const size_t bytes = t64 + sxs + q2 + fpo + qt + tsw + 5 * 256;
+  if (cudaMalloc((void **)&c->d_solve, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    c->d_solve = nullptr;
+    return fail(SNAP_ERR_OOM, "cannot allocate solve arrays");
+  }
+  c->scratch_bytes += bytes;
+  char *b = (char *)c->d_solve;
+  auto take = [&](size_t sz) {
+    char *at = b;
+    b += (sz + 255) & ~(size_t)255;
+    return at;
+  };
+  c->s_txs64 = (double *)take(t64);
+  c->s_sxs = (double *)take(sxs);
+  c->s_q2 = (double *)take(q2);
+  c->s_fpo = (double *)take(fpo);
+  c->s_qtot = take(qt);
+  c->s_txsw = c->fp32 ? (void *)take(tsw) : (void *)c->s_txs64;
+  return SNAP_OK;
+}
+
+// The solve loop: the reference's predicated loop (snap.cc:409-541) resolved
+// sequentially, for one time step (tc == null: steady state, vdelt = 0) or
+// tc->nsteps time steps with the time-edge angular flux passed from one step
+// to the next (snap.cc:288-298, 401-407, 497-498).
+int solve_impl(snap_ctx *c, const int32_t *mat, const double *qi, const double *sigt,
+               const double *slgg, const double *sigt_scale, double *flux, snap_solve_info *info,
+               cudaStream_t st, const snap_time_config *tc) {
+  if (!c || !mat || !qi || !sigt || !slgg || !flux || !info)
+    return fail(SNAP_ERR_BAD_ARG, "null argument");
+  if (info->iitm < 1 || info->oitm < 1 || !(info->epsi > 0.0))
+    return fail(SNAP_ERR_BAD_ARG, "iitm, oitm and epsi must be positive");
+  const int G = c->cfg.ng, M = c->M, nmom = c->cfg.nmom;
+  const long long C = c->C, n = (long long)G * C;
+  int rc = ensure_solve_arrays(c);
+  if (rc) return rc;
+  double *t_xs64 = c->s_txs64, *s_xs = c->s_sxs, *q2grp = c->s_q2, *fpo = c->s_fpo;
+  void *qtot = c->s_qtot, *t_xs_sw = c->s_txsw;
+  // time-dependent state: vdelt per group and the two time-edge halves
+  double *tf = nullptr, *tf_own = nullptr, *vdelt = nullptr;
+  const size_t tf_half = (size_t)8 * n * c->A;
+  if (tc) {
+    if ((rc = ensure_wide(c))) return rc;
+    if (!c->d_vdelt) {
+      if (cudaMalloc((void **)&c->d_vdelt, sizeof(double) * G) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(SNAP_ERR_OOM, "cannot allocate vdelt");
+      }
+    }
+    vdelt = c->d_vdelt;
+    if (tc->vdelt) {
+      SNAP_CUDA(cudaMemcpyAsync(vdelt, tc->vdelt, sizeof(double) * G, cudaMemcpyDeviceToDevice, st));
+    } else {
+      // Snap::initialize_velocity (snap.cc:717-739): v_g = G - g, vdelt = 2/(dt v)
+      c->h_vdelt.assign(G, 0.0);
+      for (int g = 0; g < G; ++g) c->h_vdelt[g] = 2.0 / (tc->dt * double(G - g));
+      SNAP_CUDA(cudaMemcpyAsync(vdelt, c->h_vdelt.data(), sizeof(double) * G,
+                                cudaMemcpyHostToDevice, st));
+    }
+    tf = tc->psi_t;
+    if (!tf) {
+      if (cudaMalloc((void **)&tf_own, sizeof(double) * 2 * tf_half) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(SNAP_ERR_OOM, "cannot allocate the time-edge angular flux");
+      }
+      tf = tf_own;
+    }
+    if (!tc->psi_t_initialised) SNAP_CUDA(cudaMemsetAsync(tf, 0, sizeof(double) * 2 * tf_half, st));
+  }
+#define STEP(x)                 \
+  do {                          \
+    cudaError_t e_ = (x);       \
+    if (e_ != cudaSuccess) {    \
+      rc = cuda_fail(e_, #x);   \
+      goto done;                \
+    }                           \
+  } while (0)
+  {
+    info->inner_total = info->outer_total = info->converged = info->outers_lowp = 0;
+    info->sweep_ms = info->total_ms = 0.0;
+    info->records_len = 0;
+    const double sweep_ms0 = c->sweep_ms;
+    float ms = 0.0f;
+    int rec = 0;   // entries of inners_per_outer
+    auto now_us = []() {
+      return std::chrono::duration<double, std::micro>(
+                 std::chrono::steady_clock::now().time_since_epoch())
+          .count();
+    };
+    auto log = [&](int kind, int step, int outer, int inner, int conv, double us) {
+      if (info->records && info->records_len < info->records_cap)
+        info->records[info->records_len++] = snap_iter_record{kind, step, outer, inner, conv, us};
+    };
+    STEP(cudaMemsetAsync(c->error(), 0, 2 * sizeof(int), st));
+    STEP(cudaEventRecord(c->ev0, st));
+    // per time step expansion (snap.cc:419-450); the tables do not change
+    // between time steps, so the expansion runs once
+    STEP(k_expand_xs(sigt, mat, t_xs64, G, c->cfg.nmat, C, st));
+    if (sigt_scale) STEP(k_scale_xs(t_xs64, sigt_scale, G, C, st));
+    STEP(k_expand_scat(slgg, mat, s_xs, G, c->cfg.nmat, nmom, C, st));
+    c->launches += sigt_scale ? 3 : 2;
+    if (c->fp32) {
+      STEP(k_to_f32(t_xs64, (float *)t_xs_sw, n, st));
+      ++c->launches;
+    }
+    STEP(cudaMemsetAsync(flux, 0, sizeof(double) * n * M, st));   // snap.cc:313-316
+    // precision form: BF16 tensor-core outer source while far from convergence
+    const bool lowp = c->fp32 && !(getenv("SNAP_B200_FP32_EXACT_OUTER") &&
+                                   atoi(getenv("SNAP_B200_FP32_EXACT_OUTER")) != 0) &&
+                      outer_tc_smem_bytes(G, c->cfg.nmat, nmom) <= 200 * 1024 && c->cfg.nmat <= 32;
+    // outer change above which the low-precision source is used: ten times
+    // the outer convergence tolerance, so the outer iterations that can
+    // converge run on the FP64 source
+    const double kFar = 1000.0 * info->epsi;
+    const int nsteps = tc ? tc->nsteps : 1;
+    bool even = false;
+    for (int cy = 0; cy < nsteps; ++cy) {
+      TdArgs td{};
+      if (tc) {
+        even = !even;   // snap.cc:411: in = even ? even half : odd half
+        td.vdelt = vdelt;
+        td.tf_in = even ? tf : tf + tf_half;
+        td.tf_out = even ? tf + tf_half : tf;
+        td.qim = tc->qim;
+        if (tc->qim && tc->qim_time_scaled) {
+          // MMSScale (snap.cc:451-466): source at the middle of the step
+          const double f = cy == 0 ? tc->dt * 0.5 : double(2 * cy + 1) / double(2 * cy - 1);
+          STEP(k_scale(tc->qim, f, tf_half, st));
+          ++c->launches;
+        }
+      }
+      bool far = true;
+      info->converged = 0;
+      for (int o = 0; o < info->oitm; ++o) {
+        const double t_outer = now_us();
+        const bool use_tc = lowp && far && o > 0;   // outer 0 has zero flux: q2 = qi exactly
+        c->prev_inner_df = 0.0f;                     // no stagnation test on an outer's first inner
+        if (use_tc) {
+          rc = snap_calc_outer_source_tc(c, qi, slgg, mat, flux, q2grp, st);
+          if (rc) goto done;
+          ++info->outers_lowp;
+        } else {
+          STEP(k_outer_source(qi, slgg, mat, flux, q2grp, G, c->cfg.nmat, nmom, M, C, st));
+          ++c->launches;
+        }
+        STEP(k_moment0(flux, fpo, M, n, st));                        // save_fluxes -> flux0po
+        ++c->launches;
+        bool inner_conv = false;
+        int inners = 0;
+        double t_inner = now_us();
+        for (int i = 0; i < info->iitm; ++i) {
+          int conv = 0;
+          rc = inner_iteration_impl(c, s_xs, q2grp, t_xs_sw, flux, qtot, info->epsi, &conv, st,
+                                    tc ? &td : nullptr);
+          if (rc) goto done;
+          const double t_now = now_us();
+          log(0, cy, o, i, conv, t_now - t_inner);
+          t_inner = t_now;
+          ++inners;
+          ++info->inner_total;
+          inner_conv = conv != 0;
+          if (inner_conv) break;
+        }
+        if (rec < 1024) info->inners_per_outer[rec++] = inners;
+        ++info->outer_total;
+        if (o == 0) continue;                                        // snap.cc:521-522
+        if (lowp && far) {
+          // FP64 outer residual: every scalar flux within kFar of the last outer?
+          STEP(cudaMemsetAsync(c->violations(), 0, sizeof(int), st));
+          STEP(k_test_change(flux, fpo, M, n, kFar, c->violations(), c->maxdf(), st));
+          ++c->launches;
+          int v = 0;
+          rc = read_ctrl(c, st, &v);
+          if (rc) goto done;
+          if (v == 0) far = false;
+        }
+        // convergence only on an outer iteration with the FP64 source
+        if (inner_conv && !use_tc) {
+          STEP(cudaMemsetAsync(c->violations(), 0, sizeof(int), st));
+          STEP(k_test_change(flux, fpo, M, n, 100.0 * info->epsi, c->violations(), c->maxdf(), st));
+          ++c->launches;
+          int v = 0;
+          rc = read_ctrl(c, st, &v);
+          if (rc) goto done;
+          log(1, cy, o, 0, v == 0, now_us() - t_outer);
+          if (v == 0) {
+            info->converged = 1;
+            break;
+          }
+        } else {
+          log(1, cy, o, 0, 0, now_us() - t_outer);   // the outer test fails without inner convergence
+        }
+      }
+    }
+    STEP(cudaEventRecord(c->ev1, st));
+    STEP(cudaEventSynchronize(c->ev1));
+    STEP(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    info->total_ms = ms;
+    info->sweep_ms = c->sweep_ms - sweep_ms0;
+  }
+done:
+  if (tf_own) {
+    cudaStreamSynchronize(st);
+    cudaFree(tf_own);
+  }
+#undef STEP
+  return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int snap_mms_init(snap_ctx *c, const int32_t *mat, const double *sigt, const double *slgg,
+                  double lx, double ly, double lz, int timedep, double tf, double dt,
+                  double *ref_flux, double *qim, double *qi, void *stream) {
+  if (!c || !mat || !sigt || !slgg || !ref_flux || !qim || (timedep && !qi))
+    return fail(SNAP_ERR_BAD_ARG, "null argument");
+  if (c->cfg.nmom != 1)
+    return fail(SNAP_ERR_UNSUPPORTED, "the manufactured solution has no flux moments (nmom = 1)");
+  if (!(lx > 0.0 && ly > 0.0 && lz > 0.0) || (timedep && !(dt > 0.0)))
+    return fail(SNAP_ERR_BAD_ARG, "lengths and dt must be positive");
+  cudaStream_t st = (cudaStream_t)stream;
+  MmsGeometry geo{};
+  geo.nx = c->cfg.nx;
+  geo.ny = c->cfg.ny;
+  geo.nz = c->cfg.nz;
+  geo.A = c->A;
+  geo.G = c->cfg.ng;
+  geo.nmat = c->cfg.nmat;
+  geo.lx = lx;
+  geo.ly = ly;
+  geo.lz = lz;
+  geo.timedep = timedep;
+  geo.tf = tf;
+  geo.dt = dt;
+  geo.quad[0] = c->mu.data();
+  geo.quad[1] = c->eta.data();
+  geo.quad[2] = c->xi.data();
+  double *scratch = nullptr;
+  const size_t words = mms_scratch_words(geo.nx, geo.ny, geo.nz, geo.A);
+  SNAP_CUDA(cudaMalloc((void **)&scratch, sizeof(double) * words));
+  cudaError_t e = mms_init(geo, mat, sigt, slgg, ref_flux, qim, qi, scratch, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(scratch);
+  if (e != cudaSuccess) return cuda_fail(e, "manufactured solution");
+  c->launches += timedep ? 3 : 2;
+  return SNAP_OK;
+}
+
+int snap_mms_compare(snap_ctx *c, const double *flux, const double *ref_flux, double *out,
+                     void *stream) {
+  if (!c || !flux || !ref_flux || !out) return fail(SNAP_ERR_BAD_ARG, "null argument");
+  void *scratch = nullptr;
+  SNAP_CUDA(cudaMalloc(&scratch, 3 * sizeof(double)));
+  cudaError_t e = mms_compare(flux, c->M, ref_flux, (long long)c->cfg.ng * c->C, scratch, out,
+                              (cudaStream_t)stream);
+  cudaFree(scratch);
+  if (e != cudaSuccess) return cuda_fail(e, "manufactured-solution comparison");
+  ++c->launches;
+  return SNAP_OK;
+}
+
 int snap_get_timing(snap_ctx *c, snap_timing *out, int reset) {
   if (!c || !out) return fail(SNAP_ERR_BAD_ARG, "null argument");
   out->sweep_ms = c->sweep_ms;
@@ -719,134 +1178,17 @@ int snap_test_convergence(snap_ctx *c, int kind, const double *flux, const doubl
 int snap_transport_solve(snap_ctx *c, const int32_t *mat, const double *qi, const double *sigt,
                          const double *slgg, const double *sigt_scale, double *flux,
                          snap_solve_info *info, void *stream) {
-  if (!c || !mat || !qi || !sigt || !slgg || !flux || !info)
-    return fail(SNAP_ERR_BAD_ARG, "null argument");
-  if (info->iitm < 1 || info->oitm < 1 || !(info->epsi > 0.0))
-    return fail(SNAP_ERR_BAD_ARG, "iitm, oitm and epsi must be positive");
-  cudaStream_t st = (cudaStream_t)stream;
-  const int G = c->cfg.ng, M = c->M, nmom = c->cfg.nmom;
-  const long long C = c->C, n = (long long)G * C;
-  double *t_xs64 = nullptr, *s_xs = nullptr, *q2grp = nullptr, *fpo = nullptr;
-  void *qtot = nullptr, *t_xs_sw = nullptr;
-  auto cleanup = [&]() {
-    cudaFree(t_xs64);
-    cudaFree(s_xs);
-    cudaFree(q2grp);
-    cudaFree(fpo);
-    cudaFree(qtot);
-    if (t_xs_sw != t_xs64) cudaFree(t_xs_sw);
-  };
-  if (cudaMalloc(&t_xs64, sizeof(double) * n) != cudaSuccess ||
-      cudaMalloc(&s_xs, sizeof(double) * n * nmom) != cudaSuccess ||
-      cudaMalloc(&q2grp, sizeof(double) * n * M) != cudaSuccess ||
-      cudaMalloc(&fpo, sizeof(double) * n) != cudaSuccess ||
-      cudaMalloc(&qtot, c->wsize * n * M) != cudaSuccess) {
-    cudaGetLastError();
-    cleanup();
-    return fail(SNAP_ERR_OOM, "cannot allocate solve arrays");
-  }
-  t_xs_sw = t_xs64;
-  int rc = SNAP_OK;
-#define STEP(x)                 \
-  do {                          \
-    cudaError_t e_ = (x);       \
-    if (e_ != cudaSuccess) {    \
-      rc = cuda_fail(e_, #x);   \
-      goto done;                \
-    }                           \
-  } while (0)
-  {
-    info->inner_total = info->outer_total = info->converged = info->outers_lowp = 0;
-    info->sweep_ms = info->total_ms = 0.0;
-    const double sweep_ms0 = c->sweep_ms;
-    float ms = 0.0f;
-    STEP(cudaMemsetAsync(c->error(), 0, 2 * sizeof(int), st));
-    STEP(cudaEventRecord(c->ev0, st));
-    // per time step expansion (snap.cc:419-450)
-    STEP(k_expand_xs(sigt, mat, t_xs64, G, c->cfg.nmat, C, st));
-    if (sigt_scale) STEP(k_scale_xs(t_xs64, sigt_scale, G, C, st));
-    STEP(k_expand_scat(slgg, mat, s_xs, G, c->cfg.nmat, nmom, C, st));
-    c->launches += sigt_scale ? 3 : 2;
-    if (c->fp32) {
-      if (cudaMalloc(&t_xs_sw, sizeof(float) * n) != cudaSuccess) {
-        t_xs_sw = t_xs64;
-        rc = fail(SNAP_ERR_OOM, "cannot allocate t_xs");
-        goto done;
-      }
-      STEP(k_to_f32(t_xs64, (float *)t_xs_sw, n, st));
-      ++c->launches;
-    }
-    STEP(cudaMemsetAsync(flux, 0, sizeof(double) * n * M, st));   // snap.cc:313-316
-    // precision form: BF16 tensor-core outer source while far from convergence
-    const bool lowp = c->fp32 && !(getenv("SNAP_B200_FP32_EXACT_OUTER") &&
-                                   atoi(getenv("SNAP_B200_FP32_EXACT_OUTER")) != 0) &&
-                      outer_tc_smem_bytes(G, c->cfg.nmat, nmom) <= 200 * 1024 && c->cfg.nmat <= 32;
-    // outer change above which the low-precision source is used: ten times
-    // the outer convergence tolerance, so the outer iterations that can
-    // converge run on the FP64 source
-    const double kFar = 1000.0 * info->epsi;
-    bool far = true;
-    for (int o = 0; o < info->oitm; ++o) {
-      const bool use_tc = lowp && far && o > 0;   // outer 0 has zero flux: q2 = qi exactly
-      c->prev_inner_df = 0.0f;                     // no stagnation test on an outer's first inner
-      if (use_tc) {
-        rc = snap_calc_outer_source_tc(c, qi, slgg, mat, flux, q2grp, st);
-        if (rc) goto done;
-        ++info->outers_lowp;
-      } else {
-        STEP(k_outer_source(qi, slgg, mat, flux, q2grp, G, c->cfg.nmat, nmom, M, C, st));
-        ++c->launches;
-      }
-      STEP(k_moment0(flux, fpo, M, n, st));                        // save_fluxes -> flux0po
-      ++c->launches;
-      bool inner_conv = false;
-      int inners = 0;
-      for (int i = 0; i < info->iitm; ++i) {
-        int conv = 0;
-        rc = snap_inner_iteration(c, s_xs, q2grp, t_xs_sw, flux, qtot, info->epsi, &conv, st);
-        if (rc) goto done;
-        ++inners;
-        ++info->inner_total;
-        inner_conv = conv != 0;
-        if (inner_conv) break;
-      }
-      if (o < 1024) info->inners_per_outer[o] = inners;
-      ++info->outer_total;
-      if (o == 0) continue;                                        // snap.cc:521-522
-      if (lowp && far) {
-        // FP64 outer residual: every scalar flux within kFar of the last outer?
-        STEP(cudaMemsetAsync(c->violations(), 0, sizeof(int), st));
-        STEP(k_test_change(flux, fpo, M, n, kFar, c->violations(), c->maxdf(), st));
-        ++c->launches;
-        int v = 0;
-        rc = read_ctrl(c, st, &v);
-        if (rc) goto done;
-        if (v == 0) far = false;
-      }
-      // convergence only on an outer iteration with the FP64 source
-      if (inner_conv && !use_tc) {
-        STEP(cudaMemsetAsync(c->violations(), 0, sizeof(int), st));
-        STEP(k_test_change(flux, fpo, M, n, 100.0 * info->epsi, c->violations(), c->maxdf(), st));
-        ++c->launches;
-        int v = 0;
-        rc = read_ctrl(c, st, &v);
-        if (rc) goto done;
-        if (v == 0) {
-          info->converged = 1;
-          break;
-        }
-      }
-    }
-    STEP(cudaEventRecord(c->ev1, st));
-    STEP(cudaEventSynchronize(c->ev1));
-    STEP(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
-    info->total_ms = ms;
-    info->sweep_ms = c->sweep_ms - sweep_ms0;
-  }
-done:
-  cleanup();
-#undef STEP
-  return rc;
+  return solve_impl(c, mat, qi, sigt, slgg, sigt_scale, flux, info, (cudaStream_t)stream, nullptr);
+}
+
+int snap_transport_solve_td(snap_ctx *c, const int32_t *mat, const double *qi, const double *sigt,
+                            const double *slgg, const double *sigt_scale,
+                            const snap_time_config *tc, double *flux, snap_solve_info *info,
+                            void *stream) {
+  if (!c || !tc) return fail(SNAP_ERR_BAD_ARG, "null argument");
+  if (tc->nsteps < 1 || !(tc->dt > 0.0)) return fail(SNAP_ERR_BAD_ARG, "nsteps and dt must be positive");
+  if (c->fp32) return fail(SNAP_ERR_UNSUPPORTED, "time-dependent solves run in FP64 contexts");
+  return solve_impl(c, mat, qi, sigt, slgg, sigt_scale, flux, info, (cudaStream_t)stream, tc);
 }
 
 }  // extern "C"
@@ -906,6 +1248,7 @@ extern "C" {
 int snap_record_forward(snap_ctx *c, const void *qtot, const void *t_xs, void *flux,
                         void *stream) {
   if (!c || !qtot || !t_xs || !flux) return fail(SNAP_ERR_BAD_ARG, "null argument");
+  if (c->wide_only) return fail(SNAP_ERR_UNSUPPORTED, "the adjoint needs the tiled sweep's shapes");
   cudaStream_t st = (cudaStream_t)stream;
   int rc = ensure_state(c);
   if (rc) return rc;
@@ -923,6 +1266,7 @@ int snap_record_forward(snap_ctx *c, const void *qtot, const void *t_xs, void *f
 int snap_adjoint_sweep(snap_ctx *c, const void *phi_bar, const void *t_xs, double *qtot_bar,
                        double *sigt_bar, void *stream) {
   if (!c || !phi_bar || !t_xs || !qtot_bar) return fail(SNAP_ERR_BAD_ARG, "null argument");
+  if (c->wide_only) return fail(SNAP_ERR_UNSUPPORTED, "the adjoint needs the tiled sweep's shapes");
   cudaStream_t st = (cudaStream_t)stream;
   SNAP_CUDA(cudaMemsetAsync(c->error(), 0, 2 * sizeof(int), st));
   int rc = adjoint_sweep_impl(c, phi_bar, t_xs, qtot_bar, sigt_bar, st);
@@ -940,6 +1284,7 @@ int snap_adjoint_solve(snap_ctx *c, const int32_t *mat, const double *qi, const 
     return fail(SNAP_ERR_BAD_ARG, "null argument");
   if (info->iitm < 1 || info->oitm < 1 || !(info->epsi > 0.0))
     return fail(SNAP_ERR_BAD_ARG, "iitm, oitm and epsi must be positive");
+  if (c->wide_only) return fail(SNAP_ERR_UNSUPPORTED, "the adjoint needs the tiled sweep's shapes");
   cudaStream_t st = (cudaStream_t)stream;
   const int G = c->cfg.ng, M = c->M, nmom = c->cfg.nmom;
   const long long C = c->C, n = (long long)G * C;

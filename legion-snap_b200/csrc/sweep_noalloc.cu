@@ -9,23 +9,31 @@
 //
 // How: the scratch (coefficient tables, work-item tables, tile-boundary faces,
 // progress flags, error word) lives in one file-scope __device__ array of
-// SNAP_NOALLOC_SCRATCH_BYTES bytes, which every GPU that loads this library
-// holds until the process exits.  The octants are swept one launch at a time
-// and accumulated straight into the caller's flux, so no per-octant flux
+// SNAP_NOALLOC_SCRATCH_BYTES bytes.  The octants are swept one launch at a
+// time and accumulated straight into the caller's flux, so no per-octant flux
 // slots are needed.  The host side calls no allocating CUDA or library
 // routine.
 //
 // Caveats for callers:
+//  - CUDA loads a library's code lazily by default (one module per .cu file
+//    here), so the array and the kernels' code are placed on a device when
+//    they are first used there: by the set-up call (all three array arguments
+//    NULL), or else by the first sweep.  From then on the device holds them
+//    until the process exits.  Make that set-up call, with the device
+//    current, outside any section that must not allocate.
 //  - All calls share the one array and it keeps the contents of the last
 //    call; everything that must start at zero is cleared by each call.  Calls
 //    that overlap on the GPU (other streams, other host threads) race on it.
 //  - The first call on a device looks the array's device address up with
 //    cudaGetSymbolAddress (host code cannot use the symbol itself: it is a
-//    host-side stand-in, not a device address).  Make that first call before
-//    any stream capture on that device.
+//    host-side stand-in, not a device address) and keeps it for that device.
+//    Make that first call before any stream capture on that device.  A
+//    cudaDeviceReset invalidates the kept address; calls after a reset of
+//    the device are not supported.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <mutex>
 #include <string>
 
@@ -106,13 +114,23 @@ __global__ void noalloc_items_kernel(int G, int tx_n, int ty_n, int *table, int 
 
 int fail(int code, const std::string &msg) { return set_last_error(code, msg); }
 
+// Device-side wait limit: SNAP_B200_TIMEOUT_MS as for snap_create, else 2 s.
+long long timeout_ns() {
+  long long ns = 2000000000LL;
+  if (const char *t = getenv("SNAP_B200_TIMEOUT_MS")) ns = atoll(t) * 1000000LL;
+  return ns;
+}
+
 size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
 }  // namespace
 
 extern "C" int snap_sweep_noalloc(const snap_config *cfg, const double *qtot, const double *t_xs,
                                   double *flux, void *stream) {
-  if (!cfg || !qtot || !t_xs || !flux) return fail(SNAP_ERR_BAD_ARG, "null argument");
+  if (!cfg) return fail(SNAP_ERR_BAD_ARG, "null configuration");
+  // all three arrays NULL: set-up only (load the code, look the array up)
+  const bool setup_only = !qtot && !t_xs && !flux;
+  if (!setup_only && (!qtot || !t_xs || !flux)) return fail(SNAP_ERR_BAD_ARG, "null argument");
   if (cfg->precision != SNAP_FP64) return fail(SNAP_ERR_UNSUPPORTED, "FP64 contexts only");
   if (cfg->nx < 8 || cfg->ny < 8 || cfg->nz < 1 || cfg->nx % 8 || cfg->ny % 8 || cfg->nang < 1 ||
       cfg->nang > 64 || cfg->ng < 1 || cfg->nmom < 1 || cfg->nmom > 4 || !cfg->mu || !cfg->eta ||
@@ -166,12 +184,28 @@ extern "C" int snap_sweep_noalloc(const snap_config *cfg, const double *qtot, co
   double *quad = (double *)(base + o_quad);
   int *ctl = (int *)(base + o_ctl);
 
+  if (!sweep_fp64_supported(sh))
+    return fail(SNAP_ERR_UNSUPPORTED, "no compiled sweep kernel for this shape");
   int blocks = 0, sms = 0;
   size_t smem = 0;
-  if (sweep_fp64_occupancy(sh, &blocks, &smem) != cudaSuccess || blocks < 1)
-    return fail(SNAP_ERR_UNSUPPORTED, "sweep kernel does not fit on the device");
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  e = sweep_fp64_occupancy(sh, &blocks, &smem);
+  if (e != cudaSuccess)
+    return fail(SNAP_ERR_CUDA, std::string("sweep occupancy query: ") + cudaGetErrorString(e));
+  if (blocks < 1) return fail(SNAP_ERR_UNSUPPORTED, "sweep kernel does not fit on the device");
+  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess || sms < 1)
+    return fail(SNAP_ERR_CUDA, std::string("multiprocessor count: ") + cudaGetErrorString(e));
   const int grid = (int)std::min<long long>((long long)blocks * sms, n_items);
+  if (setup_only) {
+    // the table kernels live in this file's module (loaded by the symbol
+    // lookup above); querying them makes sure their code is resident too
+    cudaFuncAttributes fa;
+    e = cudaFuncGetAttributes(&fa, noalloc_tables_kernel);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, noalloc_items_kernel);
+    if (e != cudaSuccess)
+      return fail(SNAP_ERR_CUDA, std::string("loading the table kernels: ") + cudaGetErrorString(e));
+    return SNAP_OK;
+  }
 
 #define NA_CUDA(x)                                                              \
   do {                                                                          \
@@ -205,7 +239,7 @@ extern "C" int snap_sweep_noalloc(const snap_config *cfg, const double *qtot, co
   p.tiles_y = tiles_y;
   p.n_items = (int)n_items;
   p.fixup = cfg->fixup;
-  p.timeout_ns = 2000000000LL;
+  p.timeout_ns = timeout_ns();
   p.item_table = (const int *)(base + o_tab);
   p.item_index = (const int *)(base + o_idx);
   p.qtot = qtot;

@@ -1,0 +1,249 @@
+// General FP64 sweep: one CTA per (octant, group), the CTA's threads over the
+// angles, cells walked one at a time in the upwind order of the reference's
+// CPU body (z, then y, then x fastest; sweep.cc:336-338).
+//
+// It covers what the tiled kernel (sweep.cuh) does not: any mesh extent (the
+// tiled kernel needs nx % 8 == 0 and ny % 4 == 0), up to 2048 angles per
+// octant (the tiled kernel holds at most 64 in registers; the reference's
+// time-dependent benchmark decks use 32 to 1024, input/*_1x1x1.in), the
+// time-dependent terms (vdelt * psi_t in the numerator and the denominator,
+// the time face of the fixup, psi_t out; sweep.cc:413-419, 461-468, 473-518)
+// and the manufactured per-angle source of the MMS check (sweep.cc:368-375).
+//
+// Each thread owns a fixed set of angles, so every face value it reads (the
+// x face carried in a register along the pencil, the y face of the previous
+// pencil, the z face of the previous plane, both in global scratch) was
+// written by the same thread: cells need no barrier between them except for
+// the fixup's cell-wide vote (the count of negative faces over all angles,
+// sweep.cc:425-472, a CTA-wide sum here) and the per-pencil reduction of the
+// flux moments (the angle sums of sweep.cc:565-590, combined over the warps
+// in shared memory and added with one atomic per cell and moment).
+//
+// The arithmetic follows the reference's CPU body: correctly rounded
+// division for the geometry parameter and the fixup (expxs.cc:384-385,
+// sweep.cc:499-501), and every angle of a cell recomputed in each fixup pass.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "device_util.cuh"
+#include "internal.h"
+
+namespace snapb200 {
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int MAX_THREADS = 512;
+constexpr int MAX_WARPS = MAX_THREADS / 32;
+
+template <int APT>
+__global__ void __launch_bounds__(MAX_THREADS) wide_sweep_kernel(const WideParams p) {
+  extern __shared__ double s_red[];   // [warps][nx][M] per-warp moment partials of a pencil
+  __shared__ int s_cnt[MAX_WARPS];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nwarps = blockDim.x >> 5;
+  const int o_local = blockIdx.x / p.G, g = blockIdx.x - o_local * p.G;
+  const int o = p.o_base + o_local;
+  const bool sx = o & 1, sy = (o >> 1) & 1, sz = (o >> 2) & 1;
+  const int nx = p.nx, ny = p.ny, nz = p.nz, A = p.A, M = p.M;
+  const long long C = (long long)nx * ny * nz;
+  const double *qg = p.qtot + (size_t)g * C * M;
+  const double *tg = p.t_xs + (size_t)g * C;
+  const double vd = p.td ? p.vdelt[g] : 0.0;
+  // the time terms and the time face exist only where vdelt != 0 (sweep.cc:413, 461, 473, 513)
+  const bool tt = vd != 0.0;
+  const size_t field = ((size_t)o * p.G + g) * C;   // (octant, group) field of the per-angle arrays
+  double *ypen = p.ypen + (size_t)blockIdx.x * nx * A;
+  double *zpl = p.zpl + (size_t)blockIdx.x * nx * ny * A;
+  const double *ec = p.ec + (size_t)o * M * A;
+
+  // this thread's angles and their constants
+  int ang[APT];
+  bool on[APT];
+  double cx[APT], cy[APT], cz[APT], wt[APT];
+  double xin[APT];   // x face carried along the pencil
+#pragma unroll
+  for (int k = 0; k < APT; ++k) {
+    ang[k] = tid + k * blockDim.x;
+    on[k] = ang[k] < A;
+    const int a = on[k] ? ang[k] : 0;
+    cx[k] = p.mu[a] * p.hi;
+    cy[k] = p.eta[a] * p.hj;
+    cz[k] = p.xi[a] * p.hk;
+    wt[k] = on[k] ? p.w[a] : 0.0;
+    xin[k] = 0.0;
+  }
+
+  for (int zz = 0; zz < nz; ++zz) {
+    const int z = sz ? zz : nz - 1 - zz;
+    for (int yy = 0; yy < ny; ++yy) {
+      const int y = sy ? yy : ny - 1 - yy;
+      for (int xx = 0; xx < nx; ++xx) {
+        const int x = sx ? xx : nx - 1 - xx;
+        const long long c = ((long long)z * ny + y) * nx + x;
+        const double *q = qg + c * M;
+        const double sig = __ldg(tg + c);
+        const double q0 = __ldg(q);
+        double pc[APT], psi[APT], iy[APT], iz[APT], it[APT];
+        bool neg = false;
+#pragma unroll
+        for (int k = 0; k < APT; ++k) {
+          const int a = on[k] ? ang[k] : 0;
+          // angular source (sweep.cc:354-375)
+          double s = q0;
+          for (int m = 1; m < M; ++m) s += ec[(size_t)m * A + a] * __ldg(q + m);
+          if (p.qim && on[k]) s += p.qim[(field + c) * A + a];
+          psi[k] = s;
+          if (xx == 0) xin[k] = 0.0;   // vacuum x boundary (single chunk)
+          const size_t yo = (size_t)xx * A + a, zo = ((size_t)yy * nx + xx) * A + a;
+          iy[k] = (yy == 0 || !on[k]) ? 0.0 : ypen[yo];
+          iz[k] = (zz == 0 || !on[k]) ? 0.0 : zpl[zo];
+          it[k] = (tt && on[k]) ? p.tf_in[(field + c) * A + a] : 0.0;
+          // diamond difference with the geometry parameter (expxs.cc:384-385,
+          // sweep.cc:377-423)
+          double v = s + xin[k] * cx[k];
+          v += iy[k] * cy[k];
+          v += iz[k] * cz[k];
+          if (tt) v += vd * it[k];
+          const double dinv = __drcp_rn(sig + vd + cx[k] + cy[k] + cz[k]);
+          v = on[k] ? v * dinv : 0.0;
+          pc[k] = v;
+          const double v2 = 2.0 * v;
+          neg = neg || (v2 - xin[k] < 0.0) || (v2 - iy[k] < 0.0) || (v2 - iz[k] < 0.0) ||
+                (tt && v2 - it[k] < 0.0);
+        }
+        // negative-flux fixup (sweep.cc:425-533): flags per angle and face,
+        // the count of negative faces summed over every angle of the cell,
+        // every angle recomputed until the count stops changing
+        double hx[APT], hy[APT], hz[APT], ht[APT];
+#pragma unroll
+        for (int k = 0; k < APT; ++k) hx[k] = hy[k] = hz[k] = ht[k] = 1.0;
+        if (p.fixup && __syncthreads_or(neg)) {
+          int old = 0;
+          for (int iter = 0; iter < 4 * 2048 + 4; ++iter) {
+            int cnt = 0;
+#pragma unroll
+            for (int k = 0; k < APT; ++k) {
+              if (!on[k]) continue;
+              const double v2 = 2.0 * pc[k];
+              if (v2 - xin[k] < 0.0) { hx[k] = 0.0; ++cnt; }
+              if (v2 - iy[k] < 0.0) { hy[k] = 0.0; ++cnt; }
+              if (v2 - iz[k] < 0.0) { hz[k] = 0.0; ++cnt; }
+              if (tt && v2 - it[k] < 0.0) { ht[k] = 0.0; ++cnt; }
+            }
+            cnt = __reduce_add_sync(FULL, cnt);
+            if (lane == 0) s_cnt[warp] = cnt;
+            __syncthreads();
+            int total = 0;
+            for (int w2 = 0; w2 < nwarps; ++w2) total += s_cnt[w2];
+            __syncthreads();
+            if (total == old) break;
+            old = total;
+#pragma unroll
+            for (int k = 0; k < APT; ++k) {
+              if (!on[k]) continue;
+              double v = psi[k] + 0.5 * (xin[k] * cx[k] * (1.0 + hx[k]) +
+                                         iy[k] * cy[k] * (1.0 + hy[k]) +
+                                         iz[k] * cz[k] * (1.0 + hz[k]) +
+                                         it[k] * vd * (1.0 + ht[k]));
+              const double den = (v <= 0.0) ? 0.0
+                                            : sig + cx[k] * hx[k] + cy[k] * hy[k] +
+                                                  cz[k] * hz[k] + vd * ht[k];
+              pc[k] = den < 1.0e-12 ? 0.0 : __ddiv_rn(v, den);
+            }
+          }
+        }
+        // outgoing faces (flags are all 1 without a fixup) and the moments
+        double part0 = 0.0;
+#pragma unroll
+        for (int k = 0; k < APT; ++k) {
+          if (!on[k]) continue;
+          const int a = ang[k];
+          const double v2 = 2.0 * pc[k];
+          xin[k] = (v2 - xin[k]) * hx[k];
+          ypen[(size_t)xx * A + a] = (v2 - iy[k]) * hy[k];
+          zpl[((size_t)yy * nx + xx) * A + a] = (v2 - iz[k]) * hz[k];
+          if (tt) p.tf_out[(field + c) * A + a] = (v2 - it[k]) * ht[k];
+          part0 += wt[k] * pc[k];
+        }
+        // per-warp moment partials of this cell into shared memory
+        double *red = s_red + ((size_t)warp * nx + xx) * M;
+        {
+          const double r = __shfl_xor_sync(FULL, part0, 16) + part0;
+          double r2 = r + __shfl_xor_sync(FULL, r, 8);
+          r2 += __shfl_xor_sync(FULL, r2, 4);
+          r2 += __shfl_xor_sync(FULL, r2, 2);
+          r2 += __shfl_xor_sync(FULL, r2, 1);
+          if (lane == 0) red[0] = r2;
+        }
+        for (int m = 1; m < M; ++m) {
+          double pm = 0.0;
+#pragma unroll
+          for (int k = 0; k < APT; ++k)
+            if (on[k]) pm += ec[(size_t)m * A + ang[k]] * (wt[k] * pc[k]);
+          pm += __shfl_xor_sync(FULL, pm, 16);
+          pm += __shfl_xor_sync(FULL, pm, 8);
+          pm += __shfl_xor_sync(FULL, pm, 4);
+          pm += __shfl_xor_sync(FULL, pm, 2);
+          pm += __shfl_xor_sync(FULL, pm, 1);
+          if (lane == 0) red[m] = pm;
+        }
+      }
+      // the pencil's moments: sum the warps' partials, one atomic per
+      // (cell, moment) into the flux (octants add in arrival order, as the
+      // reference's relaxed reductions do)
+      __syncthreads();
+      for (int i = tid; i < nx * M; i += blockDim.x) {
+        const int xx = i / M, m = i - xx * M;
+        double s = 0.0;
+        for (int w2 = 0; w2 < nwarps; ++w2) s += s_red[((size_t)w2 * nx + xx) * M + m];
+        const int x = sx ? xx : nx - 1 - xx;
+        const long long c = ((long long)z * ny + y) * nx + x;
+        atomicAdd(p.flux + ((size_t)g * C + c) * M + m, s);
+      }
+      __syncthreads();
+    }
+  }
+}
+
+}  // namespace
+
+int wide_apt(int A) { return A > 2 * MAX_THREADS ? 4 : A > MAX_THREADS ? 2 : 1; }
+
+int wide_threads(int A) {
+  const int apt = wide_apt(A);
+  const int t = (A + apt - 1) / apt;
+  return std::min(MAX_THREADS, ((t + 31) / 32) * 32);
+}
+
+size_t wide_smem_bytes(int A, int nx, int M) {
+  return sizeof(double) * (size_t)(wide_threads(A) / 32) * nx * M;
+}
+
+bool wide_supported(int A, int nx, int M) {
+  return A >= 1 && A <= 4 * MAX_THREADS && M >= 1 && M <= 16 &&
+         wide_smem_bytes(A, nx, M) <= 200 * 1024;
+}
+
+template <int APT>
+cudaError_t launch_apt(const WideParams &p, int n_blocks, int threads, size_t smem,
+                       cudaStream_t st) {
+  cudaError_t e = cudaFuncSetAttribute(wide_sweep_kernel<APT>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  wide_sweep_kernel<APT><<<n_blocks, threads, smem, st>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sweep_wide(const WideParams &p, int n_blocks, cudaStream_t st) {
+  if (!wide_supported(p.A, p.nx, p.M)) return cudaErrorInvalidValue;
+  const int threads = wide_threads(p.A);
+  const size_t smem = wide_smem_bytes(p.A, p.nx, p.M);
+  switch (wide_apt(p.A)) {
+    case 1: return launch_apt<1>(p, n_blocks, threads, smem, st);
+    case 2: return launch_apt<2>(p, n_blocks, threads, smem, st);
+    default: return launch_apt<4>(p, n_blocks, threads, smem, st);
+  }
+}
+
+}  // namespace snapb200

@@ -26,11 +26,24 @@ class SnapConfig(C.Structure):
                 ("ec", _dp)]
 
 
+class SnapIterRecord(C.Structure):
+    _fields_ = [("kind", C.c_int), ("time_step", C.c_int), ("outer", C.c_int),
+                ("inner", C.c_int), ("converged", C.c_int), ("us", C.c_double)]
+
+
 class SnapSolveInfo(C.Structure):
     _fields_ = [("epsi", C.c_double), ("iitm", C.c_int), ("oitm", C.c_int),
                 ("inner_total", C.c_int), ("outer_total", C.c_int), ("converged", C.c_int),
                 ("inners_per_outer", C.c_int * 1024), ("sweep_ms", C.c_double),
-                ("total_ms", C.c_double), ("outers_lowp", C.c_int)]
+                ("total_ms", C.c_double), ("outers_lowp", C.c_int),
+                ("records", C.POINTER(SnapIterRecord)), ("records_cap", C.c_int),
+                ("records_len", C.c_int)]
+
+
+class SnapTimeConfig(C.Structure):
+    _fields_ = [("nsteps", C.c_int), ("dt", C.c_double), ("vdelt", C.c_void_p),
+                ("psi_t", C.c_void_p), ("psi_t_initialised", C.c_int), ("qim", C.c_void_p),
+                ("qim_time_scaled", C.c_int)]
 
 
 class SnapTiming(C.Structure):
@@ -61,11 +74,17 @@ SIGNATURES = {
     "snap_inner_iteration": [_vp, _vp, _vp, _vp, _vp, _vp, C.c_double, _ip, _vp],
     "snap_get_timing": [_vp, C.POINTER(SnapTiming), C.c_int],
     "snap_transport_solve": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, C.POINTER(SnapSolveInfo), _vp],
+    "snap_transport_solve_td": [_vp, _vp, _vp, _vp, _vp, _vp, C.POINTER(SnapTimeConfig), _vp,
+                                C.POINTER(SnapSolveInfo), _vp],
     "snap_record_forward": [_vp, _vp, _vp, _vp, _vp],
     "snap_adjoint_sweep": [_vp, _vp, _vp, _vp, _vp, _vp],
     "snap_adjoint_solve": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                            C.POINTER(SnapSolveInfo), _vp],
     "snap_sweep_noalloc": [C.POINTER(SnapConfig), _vp, _vp, _vp, _vp],
+    "snap_inject_stall": [_vp, C.c_int],
+    "snap_mms_init": [_vp, _vp, _vp, _vp, C.c_double, C.c_double, C.c_double, C.c_int,
+                      C.c_double, C.c_double, _vp, _vp, _vp, _vp],
+    "snap_mms_compare": [_vp, _vp, _vp, _vp, _vp],
     "snap_selftest_division": [C.c_int, _vp, _vp, C.c_longlong, _vp, _vp],
     "snap_last_error": [],
 }

@@ -38,6 +38,35 @@ class Deck:
     sigt_perturb: float = 0.0     # per-cell +-fraction on sigma_t (adjoint deck)
     random_mix: int = 0           # edge of a central block with a 50 % material-2 mix
     seed: int = 1234
+    # time dependence (timedep, tf, nsteps of the deck; snap.cc:1060-1062)
+    timedep: bool = False
+    tf: float = 1.0
+    nsteps: int = 1
+    # reference decks: material and source layouts (mat_opt 0/1/2, src_opt
+    # 0/1/2/3) with the reference's own cross sections (snap.cc:571-714);
+    # None: the benchmark rule of make_problem
+    mat_opt: int | None = None
+    src_opt: int | None = None
+    # spatial chunks of the reference deck (npey, npez, ichunk); this build
+    # sweeps the whole mesh in one domain, so they only describe the deck
+    chunks: tuple = (1, 1, 1)
+
+    @property
+    def dt(self) -> float:
+        """time-step length (snap.cc:1174)"""
+        return self.tf / self.nsteps
+
+    @property
+    def h(self) -> tuple:
+        """hi, hj, hk as the reference derives them, 2 / (l / n)
+        (snap.cc:1178-1180)"""
+        return (2.0 / (self.lx / self.nx), 2.0 / (self.ly / self.ny), 2.0 / (self.lz / self.nz))
+
+    @property
+    def nmat(self) -> int:
+        """materials in the cross-section tables: one for the reference's
+        homogeneous layout (its material index space is [1, 1]), else two"""
+        return 1 if self.mat_opt == 0 else 2
 
     @property
     def cmom(self) -> int:
@@ -103,8 +132,79 @@ def scattering_matrix(ng: int, nmom: int, legendre_scale: float = 0.1) -> np.nda
     return slgg
 
 
+def reference_layout(d: Deck):
+    """InitMaterial / InitSource (init.cc:49-191): material 2 in the centre
+    block [n/4, 3n/4) (mat_opt 1) or the corner block [0, n/2) (mat_opt 2),
+    else 1; a unit source everywhere (src_opt 0), in the centre block (1) or
+    the corner block (2).  Returns mat [C] (1-based) and qi [G, C]."""
+    def block(opt, n):
+        if opt == 1:
+            return slice(n // 4, 3 * n // 4)
+        if opt == 2:
+            return slice(0, n // 2)
+        return slice(0, n)
+    mat = np.ones((d.nz, d.ny, d.nx), dtype=np.int32)
+    if d.mat_opt in (1, 2):
+        mat[block(d.mat_opt, d.nz), block(d.mat_opt, d.ny), block(d.mat_opt, d.nx)] = 2
+    src = np.zeros((d.nz, d.ny, d.nx))
+    if d.src_opt in (0, 1, 2):
+        src[block(d.src_opt, d.nz), block(d.src_opt, d.ny), block(d.src_opt, d.nx)] = 1.0
+    qi = np.broadcast_to(src.reshape(1, d.cells), (d.ng, d.cells)).copy()
+    return mat.reshape(d.cells), qi
+
+
+def reference_cross_sections(ng: int, nmom: int, two_materials: bool):
+    """Snap::initialize_scattering (snap.cc:571-714): sigma_t, sigma_a and
+    sigma_s fall by 0.01 and 0.005 per group from (1, 0.5, 0.5) in material 1
+    and (2, 0.8, 1.2) in material 2; slgg splits sigma_s of each source group
+    into in-group, up-scatter and down-scatter shares (0.2 / 0.1 / 0.7 in
+    material 1, 0.5 / 0.1 / 0.4 in material 2; the first group keeps 0.3 (0.6)
+    in-group, the last 0.9), Legendre orders scaled by 0.1 then 0.5 (material
+    1) or 0.8 then 0.6 (material 2).  Returns sigt [G, nmat] and
+    slgg [G_to, nmat, G_from, nmom] in this package's layout."""
+    nmat = 2 if two_materials else 1
+    sigt = np.zeros((ng, nmat))
+    sigs = np.zeros((ng, nmat))
+    base = [(1.0, 0.5), (2.0, 1.2)]
+    for m in range(nmat):
+        sigt[0, m], sigs[0, m] = base[m]
+        for g in range(1, ng):
+            sigt[g, m] = 0.01 * sigt[g - 1, m]
+            sigs[g, m] = 0.005 * sigs[g - 1, m]
+    slgg = np.zeros((ng, nmat, ng, nmom))
+    shares = [(0.2, 0.3, 0.7, 0.9), (0.5, 0.6, 0.4, 0.9)]   # in-group, first group, down, last group
+    for m in range(nmat):
+        if ng == 1:
+            slgg[0, m, 0, 0] = sigs[0, m]
+            continue
+        ingroup, first, down, last = shares[m]
+        for g in range(ng):                       # g: source group
+            slgg[g, m, g, 0] = ingroup * sigs[g, m]
+            if g > 0:
+                t = 1.0 / g
+                for g2 in range(g):
+                    slgg[g2, m, g, 0] = 0.1 * sigs[g, m] * t
+            else:
+                slgg[g, m, g, 0] = first * sigs[g, m]
+            if g < ng - 1:
+                t = 1.0 / (ng - (g + 1))
+                for g2 in range(g + 1, ng):
+                    slgg[g2, m, g, 0] = down * sigs[g, m] * t
+            else:
+                slgg[g, m, g, 0] = last * sigs[g, m]
+    scale = [(0.1, 0.5), (0.8, 0.6)]
+    for m in range(nmat):
+        for l in range(1, nmom):
+            slgg[:, m, :, l] = (scale[m][0] if l == 1 else scale[m][1]) * slgg[:, m, :, l - 1]
+    return sigt, slgg
+
+
 def make_problem(d: Deck) -> dict:
     """Material map, fixed source and cross-section tables for a deck."""
+    if d.mat_opt is not None:
+        mat, qi = reference_layout(d)
+        sigt, slgg = reference_cross_sections(d.ng, d.nmom, d.mat_opt != 0)
+        return dict(mat=mat, qi=qi, sigt=sigt, slgg=slgg, nmat=sigt.shape[1])
     C = d.cells
     mat = np.ones((d.nz, d.ny, d.nx), dtype=np.int32)
     src = np.zeros((d.nz, d.ny, d.nx), dtype=np.float64)

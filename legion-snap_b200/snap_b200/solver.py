@@ -54,10 +54,9 @@ class Snap:
         self._host = [np.ascontiguousarray(a, dtype=np.float64) for a in (mu, eta, xi, w, ec)]
         dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))  # noqa: E731
         cfg = abi.SnapConfig(
-            deck.nx, deck.ny, deck.nz, deck.nang, deck.ng, deck.nmom, 2, int(deck.fixup),
+            deck.nx, deck.ny, deck.nz, deck.nang, deck.ng, deck.nmom, deck.nmat, int(deck.fixup),
             abi.SNAP_FP64 if precision == "fp64" else abi.SNAP_FP32,
-            2.0 * deck.nx / deck.lx, 2.0 * deck.ny / deck.ly, 2.0 * deck.nz / deck.lz,
-            *(dp(a) for a in self._host))
+            *deck.h, *(dp(a) for a in self._host))
         handle = C.c_void_p()
         with torch.cuda.device(self.device):
             abi.check(self.lib.snap_create(C.byref(cfg), device, C.byref(handle)))
@@ -249,15 +248,43 @@ class Snap:
         info.iitm = d.iitm if iitm is None else iitm
         info.oitm = d.oitm if oitm is None else oitm
         scale = dprob.get("sigt_scale")
-        abi.check(self.lib.snap_transport_solve(
-            self.handle, _ptr(dprob["mat"]), _ptr(dprob["qi"]), _ptr(dprob["sigt"]),
-            _ptr(dprob["slgg"]), _ptr(scale) if scale is not None else None, _ptr(flux),
-            C.byref(info), _stream()))
+        cap = 4096
+        recs = (abi.SnapIterRecord * cap)()
+        info.records = C.cast(recs, C.POINTER(abi.SnapIterRecord))
+        info.records_cap = cap
+        args = (self.handle, _ptr(dprob["mat"]), _ptr(dprob["qi"]), _ptr(dprob["sigt"]),
+                _ptr(dprob["slgg"]), _ptr(scale) if scale is not None else None)
+        if d.timedep or "qim" in dprob:
+            # time stepping, or a manufactured per-angle source (a steady
+            # MMS deck runs one step with vdelt = 0)
+            tc = abi.SnapTimeConfig()
+            tc.nsteps = d.nsteps if d.timedep else 1
+            tc.dt = d.dt
+            if not d.timedep:
+                vzero = torch.zeros(d.ng, dtype=torch.float64, device=self.device)
+                tc.vdelt = _ptr(vzero)
+            tc.qim = _ptr(dprob["qim"]) if "qim" in dprob else None
+            tc.qim_time_scaled = 1 if "qim" in dprob else 0
+            if "psi_t" in dprob:
+                tc.psi_t = _ptr(dprob["psi_t"])
+                tc.psi_t_initialised = 1
+            abi.check(self.lib.snap_transport_solve_td(*args, C.byref(tc), _ptr(flux),
+                                                       C.byref(info), _stream()))
+        else:
+            abi.check(self.lib.snap_transport_solve(*args, _ptr(flux), C.byref(info), _stream()))
+        n_rec = min(info.outer_total, 1024)
         rec = dict(inner_total=info.inner_total, outer_total=info.outer_total,
                    converged=bool(info.converged),
-                   inners_per_outer=list(info.inners_per_outer[:info.outer_total]),
-                   total_ms=info.total_ms, sweep_ms=info.sweep_ms, outers_lowp=info.outers_lowp)
+                   inners_per_outer=list(info.inners_per_outer[:n_rec]),
+                   total_ms=info.total_ms, sweep_ms=info.sweep_ms, outers_lowp=info.outers_lowp,
+                   records=_records(info))
         return flux, rec
+
+
+def _records(info) -> list:
+    return [dict(kind="inner" if r.kind == 0 else "outer", time_step=r.time_step, outer=r.outer,
+                 inner=r.inner, converged=bool(r.converged), us=r.us)
+            for r in info.records[:info.records_len]]
 
 
 def fp64_finish(deck: Deck, dprob: dict, flux: torch.Tensor, outers: int = 1, device: int = 0):

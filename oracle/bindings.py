@@ -54,11 +54,14 @@ def build():
 class Oracle:
     """Our FP64 restatement of the reference's CPU task bodies."""
 
-    def __init__(self, deck, prob=None):
+    def __init__(self, deck, prob=None, threads: int = 1):
         lib_path = HERE / "liboracle.so"
         if not lib_path.exists():
             build()
         self.lib = C.CDLL(str(lib_path))
+        # groups are independent sweeps: spread them over host threads (the
+        # result does not depend on the thread count)
+        self.lib.oracle_set_threads(int(threads))
         self.deck = deck
         d = deck
         self.mu = np.zeros(d.nang)
@@ -68,9 +71,8 @@ class Oracle:
         self.ec = np.zeros((8, d.cmom, d.nang))
         self.lib.oracle_quadrature(d.nang, d.nmom, _d(self.mu), _d(self.eta), _d(self.xi),
                                    _d(self.w), _d(self.ec))
-        self.geom = _Geom(d.nx, d.ny, d.nz, d.nang, d.ng, d.nmom, d.cmom, 2, int(d.fixup),
-                          2.0 * d.nx / d.lx, 2.0 * d.ny / d.ly, 2.0 * d.nz / d.lz,
-                          _d(self.mu), _d(self.eta), _d(self.xi), _d(self.w), _d(self.ec))
+        self.geom = _Geom(d.nx, d.ny, d.nz, d.nang, d.ng, d.nmom, d.cmom, d.nmat, int(d.fixup),
+                          *d.h, _d(self.mu), _d(self.eta), _d(self.xi), _d(self.w), _d(self.ec))
         self.prob = prob
 
     @property
@@ -147,11 +149,21 @@ class RefSnap:
         self.lib = C.CDLL(str(self.PATH))
         self.lib.snapref_solve.restype = C.c_double
         self.deck = deck
-        rc = self.lib.snapref_configure(deck.nx, deck.ny, deck.nz, deck.nang, deck.ng, deck.nmom,
-                                        1, C.c_double(deck.epsi), deck.iitm, deck.oitm,
-                                        int(deck.fixup))
+        if deck.mat_opt is None and not deck.timedep:
+            rc = self.lib.snapref_configure(deck.nx, deck.ny, deck.nz, deck.nang, deck.ng,
+                                            deck.nmom, 1, C.c_double(deck.epsi), deck.iitm,
+                                            deck.oitm, int(deck.fixup))
+        else:
+            # a reference deck: its layouts, lengths and time stepping
+            mat_opt = 1 if deck.mat_opt is None else deck.mat_opt
+            src_opt = 1 if deck.src_opt is None else deck.src_opt
+            rc = self.lib.snapref_configure_deck(
+                deck.nx, deck.ny, deck.nz, C.c_double(deck.lx), C.c_double(deck.ly),
+                C.c_double(deck.lz), deck.nang, deck.ng, deck.nmom, C.c_double(deck.epsi),
+                deck.iitm, deck.oitm, int(deck.fixup), int(deck.timedep), C.c_double(deck.tf),
+                deck.nsteps, mat_opt, src_opt)
         if rc != 0:
-            raise RuntimeError(f"snapref_configure failed: {rc}")
+            raise RuntimeError(f"reference configuration failed: {rc}")
 
     def quadrature(self):
         n = self.deck.nang
@@ -179,17 +191,25 @@ class RefSnap:
         if nthreads is None:
             nthreads = os.cpu_count() or 1
         flux = np.zeros((d.ng, d.cells))
-        info = np.zeros(3 + d.oitm, dtype=np.int32)
+        mms = np.zeros(3)                       # MMS compare: max, min, sum of |flux/ref - 1|
+        ref_flux = np.zeros((d.ng, d.cells))    # MMS reference flux (scaled as compared)
+        steps = d.nsteps if d.timedep else 1
+        info = np.zeros(3 + d.oitm * steps, dtype=np.int32)
         sweep_s = C.c_double(0.0)
         secs = self.lib.snapref_solve(_i(prob["mat"]), _d(prob["qi"]),
                                       _d(np.ascontiguousarray(prob["sigt"])),
-                                      _d(np.ascontiguousarray(prob["slgg"])), 2, variant, nthreads,
+                                      _d(np.ascontiguousarray(prob["slgg"])),
+                                      int(prob.get("nmat", 2)), variant, nthreads,
                                       max_inners, _d(flux), info.ctypes.data_as(_ip),
-                                      C.byref(sweep_s))
+                                      C.byref(sweep_s), _d(mms), _d(ref_flux))
         if secs < 0:
             raise RuntimeError(f"snapref_solve failed: {secs}")
         rec = dict(inner_total=int(info[0]), outer_total=int(info[1]), converged=bool(info[2]),
                    inners_per_outer=[int(x) for x in info[3:3 + info[1]]],
                    seconds=secs, sweep_seconds=sweep_s.value, variant=variant,
                    nthreads=nthreads)
+        if d.src_opt == 3:
+            rec["mms"] = dict(max=float(mms[0]), min=float(mms[1]), sum=float(mms[2]),
+                              avg=float(mms[2]) / (d.cells * d.ng))
+            rec["ref_flux"] = ref_flux
         return flux, rec

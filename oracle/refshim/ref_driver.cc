@@ -22,6 +22,7 @@
 #include "inner.h"
 #include "expxs.h"
 #include "init.h"
+#include "mms.h"
 
 #include <atomic>
 #include <chrono>
@@ -349,9 +350,50 @@ int snapref_configure(int nx, int ny, int nz, int nang, int ng, int nmom, int tw
   Snap::max_outer_iters = oitm;
   Snap::flux_fixup = fixup != 0;
   Snap::time_dependent = false;
+  Snap::total_sim_time = 0.0;
+  Snap::num_steps = 1;
+  Snap::dt = 0.0;
   Snap::material_layout = two_materials ? Snap::CENTER_LAYOUT : Snap::HOMOGENEOUS_LAYOUT;
   Snap::source_layout = Snap::CENTER_SOURCE;
   Snap::num_corners = 8;
+  derive_globals();
+  return 0;
+}
+
+/* Sets every deck parameter the solve path reads (the fields parse_arguments
+ * fills, snap.cc:1032-1168), single spatial chunk.  mat_opt: 0 homogeneous,
+ * 1 center, 2 corner; src_opt: 0 everywhere, 1 center, 2 corner. */
+int snapref_configure_deck(int nx, int ny, int nz, double lx, double ly, double lz, int nang,
+                           int ng, int nmom, double epsi, int iitm, int oitm, int fixup,
+                           int timedep, double tf, int nsteps, int mat_opt, int src_opt) {
+  if (nmom != 1) return -1;
+  if (mat_opt < 0 || mat_opt > 2 || src_opt < 0 || src_opt > 3 || nsteps < 1) return -2;
+  Snap::num_dims = 3;
+  Snap::nx = Snap::nx_per_chunk = nx;
+  Snap::ny = Snap::ny_per_chunk = ny;
+  Snap::nz = Snap::nz_per_chunk = nz;
+  Snap::nx_chunks = Snap::ny_chunks = Snap::nz_chunks = 1;
+  Snap::lx = lx;
+  Snap::ly = ly;
+  Snap::lz = lz;
+  Snap::num_angles = nang;
+  Snap::num_groups = ng;
+  Snap::num_moments = nmom;
+  Snap::convergence_eps = epsi;
+  Snap::max_inner_iters = iitm;
+  Snap::max_outer_iters = oitm;
+  Snap::flux_fixup = fixup != 0;
+  Snap::time_dependent = timedep != 0;
+  Snap::total_sim_time = tf;
+  Snap::num_steps = nsteps;
+  static const Snap::MaterialLayout ml[3] = {Snap::HOMOGENEOUS_LAYOUT, Snap::CENTER_LAYOUT,
+                                             Snap::CORNER_LAYOUT};
+  static const Snap::SourceLayout sl[4] = {Snap::EVERYWHERE_SOURCE, Snap::CENTER_SOURCE,
+                                           Snap::CORNER_SOURCE, Snap::MMS_SOURCE};
+  Snap::material_layout = ml[mat_opt];
+  Snap::source_layout = sl[src_opt];
+  Snap::num_corners = 8;
+  Snap::dt = tf / double(nsteps);   /* snap.cc:1174 */
   derive_globals();
   return 0;
 }
@@ -374,8 +416,11 @@ int snapref_init_layout(int32_t *mat_out, double *qi_out) {
   SnapArray<3> qi(p.sim_is, ip3, p.group_fs, nullptr, &g_runtime, "qi");
   int *m = (int *)store_of(mat).mem;
   for (size_t c = 0; c < store_of(mat).volume; c++) m[c] = 1; /* snap.cc:325 */
-  InitMaterial im(snap, mat);
-  execute<void>(im, &InitMaterial::cpu_implementation);
+  /* snap.cc:345-349: InitMaterial runs for the non-homogeneous layouts only */
+  if (Snap::material_layout != Snap::HOMOGENEOUS_LAYOUT) {
+    InitMaterial im(snap, mat);
+    execute<void>(im, &InitMaterial::cpu_implementation);
+  }
   InitSource is(snap, qi);
   execute<void>(is, &InitSource::cpu_implementation);
   const size_t C = store_of(mat).volume;
@@ -389,16 +434,19 @@ int snapref_init_layout(int32_t *mat_out, double *qi_out) {
  *   mat [C] (1-based), qi [G][C], sigt [G][nmat], slgg [G_to][nmat][G_from][nmom]
  *   variant: 0 scalar, 1 SSE, 2 AVX sweep body
  *   flux_out [G][C]; info[0] inner total, info[1] outer total, info[2]
- *   converged, info[3+o] inner iterations of outer o (o < oitm)
+ *   converged (last time step), info[3+r] inner iterations of the r-th
+ *   outer iteration over all time steps (r < oitm * nsteps)
  *   max_inners_total > 0 stops after that many inner iterations (timing).
  * Returns seconds spent, or a negative error.
  */
 double snapref_solve(const int32_t *mat_in, const double *qi_in, const double *sigt_in,
                      const double *slgg_in, int nmat, int variant, int nthreads,
                      int max_inners_total, double *flux_out, int *info,
-                     double *sweep_seconds) {
+                     double *sweep_seconds, double *mms_out, double *ref_flux_out) {
   SweepImpl sweep_impl = pick_sweep(variant);
   if (!sweep_impl) return -1.0;
+  /* info holds 3 + oitm * nsteps entries: outer iterations of every step */
+  const int max_records = Snap::max_outer_iters * Snap::num_steps;
   if (variant == 1 && Snap::num_angles % 2) return -2.0;
   if (variant == 2 && Snap::num_angles % 4) return -2.0;
   const int G = Snap::num_groups;
@@ -428,12 +476,45 @@ double snapref_solve(const int32_t *mat_in, const double *qi_in, const double *s
   SnapArray<3> s_xs(p.sim_is, ip3, p.moment_fs, nullptr, &g_runtime, "s_xs");
   SnapArray<1> vdelt(p.point_is, ip1, p.group_fs, nullptr, &g_runtime, "vdelt");
   SnapArray<3> dinv(p.sim_is, ip3, p.angle_fs, nullptr, &g_runtime, "dinv");
-  /* steady state: the time-flux and MMS regions are named by the sweep's
-   * region requirements but never dereferenced (sweep.cc:413, :369) */
-  g_phantom_next = true;
-  SnapArray<3> tf(p.sim_is, ip3, p.angle_fs, nullptr, &g_runtime, "time flux");
-  SnapArray<3> qim(p.sim_is, ip3, p.angle_fs, nullptr, &g_runtime, "qim");
+  /* the MMS region is named by the sweep's region requirements but never
+   * dereferenced outside MMS decks (sweep.cc:369); the time-edge angular
+   * flux is real storage in time-dependent decks only (sweep.cc:413) */
+  const bool td = Snap::time_dependent;
+  const bool mms = Snap::source_layout == Snap::MMS_SOURCE;
+  g_phantom_next = !mms;
+  std::vector<SnapArray<3> *> qim(8);
+  for (int i = 0; i < 8; i++)
+    qim[i] = new SnapArray<3>(p.sim_is, ip3, p.angle_fs, nullptr, &g_runtime, "qim");
+  SnapArray<3> ref_flux(p.sim_is, ip3, p.group_fs, nullptr, &g_runtime, "ref_flux");
+  SnapArray<3> ref_fluxm(p.sim_is, ip3, p.flux_moment_fs, nullptr, &g_runtime, "ref_fluxm");
+  SnapArray<1> vel(p.point_is, ip1, p.group_fs, nullptr, &g_runtime, "vel");
+  g_phantom_next = !td;
+  std::vector<SnapArray<3> *> tf_even(8), tf_odd(8);
+  for (int i = 0; i < 8; i++) {
+    tf_even[i] = new SnapArray<3>(p.sim_is, ip3, p.angle_fs, nullptr, &g_runtime, "tf even");
+    tf_odd[i] = new SnapArray<3>(p.sim_is, ip3, p.angle_fs, nullptr, &g_runtime, "tf odd");
+  }
   g_phantom_next = false;
+  struct TfFree {
+    std::vector<SnapArray<3> *> &a, &b;
+    ~TfFree() {
+      for (auto *x : a) delete x;
+      for (auto *x : b) delete x;
+    }
+  } tf_free{tf_even, tf_odd};
+  struct QimFree {
+    std::vector<SnapArray<3> *> &a;
+    ~QimFree() {
+      for (auto *x : a) delete x;
+    }
+  } qim_free{qim};
+  /* Snap::initialize_velocity (snap.cc:717-739): v_g = G - g,
+   * vdelt = 2 / (dt v_g) when time dependent, else 0 */
+  for (int g = 0; g < G; g++) {
+    const double v = double(G - g);
+    ((double *)store_of(vdelt).field_base(g))[0] = td ? 2.0 / (Snap::dt * v) : 0.0;
+    if (mms) ((double *)store_of(vel).field_base(g))[0] = v;
+  }
 
   const size_t C = store_of(flux0).volume;
   if (nmat != (int)store_of(sigt).volume) return -3.0;
@@ -468,12 +549,41 @@ double snapref_solve(const int32_t *mat_in, const double *qi_in, const double *s
     execute<void>(gp, &CalculateGeometryParam::cpu_implementation);
   }
 
+  /* the manufactured solution (snap.cc:373-388): reference flux, the
+   * per-corner angular source and, time dependent, qi = flux / v with the
+   * reference flux scaled to the middle of the last step */
+  if (mms) {
+    MMSInitFlux mf(snap, ref_flux, ref_fluxm);
+    execute<void>(mf, &MMSInitFlux::cpu_implementation);
+    for (int i = 0; i < 8; i++) {
+      MMSInitSource ms(snap, ref_flux, ref_fluxm, mat, sigt, slgg, *qim[i], i);
+      execute<void>(ms, &MMSInitSource::cpu_implementation);
+    }
+    if (td) {
+      MMSInitTimeDependent mt(snap, vel, ref_flux, qi);
+      execute<void>(mt, &MMSInitTimeDependent::cpu_implementation);
+    }
+  }
+
   Predicate pred;
   const Future true_future = Future::from_value<bool>(nullptr, true);
-  int inner_total = 0, outer_total = 0, converged = 0;
+  int inner_total = 0, outer_total = 0, converged = 0, records = 0;
   double t_sweep = 0.0;
   const auto t0 = std::chrono::steady_clock::now();
   bool stop = false;
+  bool even_time_step = false;
+  for (int cy = 0; cy < Snap::num_steps && !stop; ++cy) {
+  even_time_step = !even_time_step;   /* snap.cc:411 */
+  if (mms) { /* snap.cc:451-466 */
+    const double f = cy == 0 ? Snap::dt * 0.5 : double(2 * cy + 1) / double(2 * cy - 1);
+    for (int i = 0; i < 8; i++) {
+      MMSScale sc(snap, *qim[i], f);
+      execute<void>(sc, &MMSScale::cpu_implementation);
+    }
+  }
+  std::vector<SnapArray<3> *> &tf_in = even_time_step ? tf_even : tf_odd;
+  std::vector<SnapArray<3> *> &tf_out = even_time_step ? tf_odd : tf_even;
+  converged = 0;
   for (int otno = 0; otno < Snap::max_outer_iters && !stop; ++otno) {
     CalcOuterSource os(snap, pred, qi, slgg, mat, q2grp0, q2grpm, flux0, fluxm);
     execute<void>(os, &CalcOuterSource::cpu_implementation);
@@ -497,8 +607,9 @@ double snapref_solve(const int32_t *mat_in, const double *qi_in, const double *s
         const int corner = t / G, g = t % G;
         int ghost_offsets[3] = {0, 0, 0};
         for (int i = 0; i < 3; i++) ghost_offsets[i] = (corner & (1 << i)) >> i;
-        MiniKBATask k(snap, pred, flux0, fluxm, qtot, vdelt, dinv, t_xs, tf, tf, qim, flux_xy,
-                      flux_yz, flux_xz, g, g, corner, ghost_offsets);
+        MiniKBATask k(snap, pred, flux0, fluxm, qtot, vdelt, dinv, t_xs, *tf_in[corner],
+                      *tf_out[corner], *qim[corner], flux_xy, flux_yz, flux_xz, g, g, corner,
+                      ghost_offsets);
         execute<void>(k, sweep_impl);
       });
       t_sweep += std::chrono::duration<double>(std::chrono::steady_clock::now() - ts).count();
@@ -513,7 +624,8 @@ double snapref_solve(const int32_t *mat_in, const double *qi_in, const double *s
       if (max_inners_total > 0 && inner_total >= max_inners_total) { stop = true; break; }
       if (inner_conv) break;
     }
-    if (info && otno < Snap::max_outer_iters) info[3 + otno] = inners;
+    if (info && records < max_records) info[3 + records] = inners;
+    records++;
     outer_total++;
     if (stop) break;
     if (otno == 0) continue;
@@ -525,8 +637,15 @@ double snapref_solve(const int32_t *mat_in, const double *qi_in, const double *s
     }
     if (conv) { converged = 1; break; }
   }
+  }
   const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   if (flux_out) memcpy(flux_out, store_of(flux0).mem, C * G * sizeof(double));
+  if (mms) { /* snap.cc:542-560 */
+    MMSCompare cmp(snap, flux0, ref_flux);
+    const MomentTriple r = execute<MomentTriple>(cmp, &MMSCompare::cpu_implementation);
+    if (mms_out) for (int i = 0; i < 3; i++) mms_out[i] = r[i];
+    if (ref_flux_out) memcpy(ref_flux_out, store_of(ref_flux).mem, C * G * sizeof(double));
+  }
   if (info) { info[0] = inner_total; info[1] = outer_total; info[2] = converged; }
   if (sweep_seconds) *sweep_seconds = t_sweep;
   return secs;

@@ -1,0 +1,158 @@
+"""The reference's own input decks (input/*.in, parsed by snap_b200.input_deck)
+solved through the C ABI and compared with the reference's CPU task bodies
+(oracle/_ref, built from the reference sources) on the same deck: steady-state
+decks of several chunk layouts, and time-dependent decks (vdelt, the
+time-edge angular flux, its fixup face) of 32 to 1024 angles per octant.
+Shapes outside the tiled sweep (6^3 mesh, more than 64 angles) run the
+general kernel.  FP64: scalar flux within 1e-12 relative, iteration records
+identical."""
+import dataclasses
+import os
+import pathlib
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = [
+    pytest.mark.gpu,
+    pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA device"),
+]
+
+from oracle.bindings import Oracle, RefSnap  # noqa: E402
+from snap_b200 import input_deck as D  # noqa: E402
+from snap_b200 import problem as P  # noqa: E402
+
+TOL = 1e-12
+DECKS = pathlib.Path(__file__).resolve().parent / "decks"
+needs_ref = pytest.mark.skipif(not RefSnap.available(), reason="reference build not present")
+
+
+def rel_err(a, b):
+    return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300)))
+
+
+def solve_both(d):
+    from snap_b200.solver import Snap
+    prob = P.make_problem(d)
+    snap = Snap(d)
+    flux, rec = snap.transport_solve(snap.device_problem(prob))
+    ref, rref = RefSnap(d).solve(prob, nthreads=os.cpu_count() or 1)
+    snap.close()
+    return flux[..., 0].cpu().numpy(), rec, ref, rref
+
+
+@needs_ref
+@pytest.mark.parametrize("name", ["simple.in", "test.in", "base.in"])
+def test_steady_state_deck_matches_reference(name):
+    """simple.in (32^3, one group), test.in (32^3, 4 groups, 2x2x2 chunks),
+    base.in (6^3, general kernel)."""
+    d = D.parse_deck(DECKS / name).deck
+    phi, rec, ref, rref = solve_both(d)
+    assert rel_err(phi, ref) < TOL
+    assert rec["inners_per_outer"] == rref["inners_per_outer"]
+    assert rec["converged"] == rref["converged"]
+
+
+@needs_ref
+@pytest.mark.parametrize("name,steps", [("tiny_512_1x1x1.in", None), ("small_512_1x1x1.in", None),
+                                        ("medium_512_1x1x1.in", 4), ("huge_512_1x1x1.in", 2)])
+def test_time_dependent_deck_matches_reference(name, steps):
+    """Time-dependent decks, 32 / 128 / 256 / 1024 angles per octant (the
+    larger ones on fewer time steps to bound the CPU reference's time): the
+    scalar flux after the last step and the outer/inner record of every
+    step."""
+    d = D.parse_deck(DECKS / name).deck
+    if steps:
+        d = dataclasses.replace(d, nsteps=steps, tf=d.dt * steps)
+    phi, rec, ref, rref = solve_both(d)
+    assert rel_err(phi, ref) < TOL
+    assert rec["inners_per_outer"] == rref["inners_per_outer"]
+    assert rec["inner_total"] == rref["inner_total"]
+
+
+@needs_ref
+def test_time_dependent_2048_angles():
+    """The largest angle count the general kernel takes (four angles per
+    thread) on a small time-dependent problem."""
+    d = P.Deck(4, 4, 4, nang=2048, ng=2, nmom=1, epsi=1e-4, iitm=3, oitm=4, lx=0.6, ly=0.6,
+               lz=0.6, timedep=True, tf=1.0, nsteps=2, mat_opt=1, src_opt=1)
+    phi, rec, ref, rref = solve_both(d)
+    assert rel_err(phi, ref) < TOL
+    assert rec["inners_per_outer"] == rref["inners_per_outer"]
+
+
+def test_general_kernel_multimoment_matches_oracle():
+    """A ragged mesh (the tiled kernel needs nx % 8 == 0) with nmom = 3:
+    the general kernel's moment expansion and accumulation against the
+    oracle."""
+    from snap_b200.solver import Snap
+    d = P.Deck(12, 10, 6, nang=20, ng=3, nmom=3, epsi=1e-6, iitm=3, oitm=3)
+    prob = P.make_problem(d)
+    ref, rref = Oracle(d).solve(prob)
+    snap = Snap(d)
+    flux, rec = snap.transport_solve(snap.device_problem(prob))
+    got = flux.cpu().numpy()
+    assert rel_err(got[..., 0], ref[..., 0]) < TOL
+    scale = np.abs(ref).reshape(-1, d.cmom).max(axis=0)
+    assert float((np.abs(got - ref).reshape(-1, d.cmom).max(axis=0) / scale).max()) < TOL
+    assert rec["inners_per_outer"] == rref["inners_per_outer"]
+    snap.close()
+
+
+def test_convergence_log_lines():
+    """The iteration records of a solve print as the reference's convergence
+    log (one line per inner iteration, per outer test, per time step)."""
+    import io
+    from snap_b200.solver import Snap
+    d = D.parse_deck(DECKS / "tiny_512_1x1x1.in").deck
+    d = dataclasses.replace(d, nsteps=2, tf=d.dt * 2)
+    snap = Snap(d)
+    _, rec = snap.transport_solve(snap.device_problem(P.make_problem(d)))
+    out = io.StringIO()
+    D.convergence_log(rec["records"], out)
+    lines = out.getvalue().splitlines()
+    assert sum(line.startswith("Inner loop") for line in lines) == rec["inner_total"]
+    assert sum(line.startswith("Time step") for line in lines) == 2
+    assert "SNAP Execution Summary" in lines
+    snap.close()
+
+
+# ---------------------------------------------------------------- MMS
+@needs_ref
+@pytest.mark.parametrize("timedep", [True, False], ids=["mms.in", "steady"])
+def test_mms_deck_matches_reference(timedep):
+    """input/mms.in (16^3, 16 angles, 4 groups, 2 time steps, manufactured
+    source) against the reference's own MMS tasks and sweep: the solved flux
+    to 1e-12, the iteration record, and the comparison (max, min, sum of
+    |flux/ref - 1|).  The reference's own result passes its max threshold
+    (0.1) on this deck; its average (2.6e-3) is above the 1e-3 threshold, a
+    discretisation error of the 16^3 mesh (see the refinement test)."""
+    from snap_b200.mms import MAX_LIMIT, mms_solve
+    d = D.parse_deck(DECKS / "mms.in").deck
+    if not timedep:
+        d = dataclasses.replace(d, timedep=False, nsteps=1)
+    flux, rec, res, ref_flux = mms_solve(d)
+    rflux, rrec = RefSnap(d).solve(P.make_problem(d), nthreads=os.cpu_count() or 1)
+    assert rel_err(flux[..., 0].cpu().numpy(), rflux) < TOL
+    assert rel_err(ref_flux.cpu().numpy(), rrec["ref_flux"]) < TOL
+    assert rec["inners_per_outer"] == rrec["inners_per_outer"]
+    for key in ("max", "sum"):
+        assert abs(res[key] - rrec["mms"][key]) <= 1e-9 * abs(rrec["mms"][key])
+    if timedep:
+        assert res["max"] < MAX_LIMIT
+
+
+def test_mms_error_falls_second_order():
+    """The manufactured solution's average error shrinks about fourfold per
+    halving of the cell size (8^3 -> 16^3 -> 32^3, the mms.in deck
+    otherwise), the order of the diamond-difference scheme; at 32^3 it is
+    within the reference's 1e-3 threshold."""
+    from snap_b200.mms import AVG_LIMIT, mms_solve
+    d0 = D.parse_deck(DECKS / "mms.in").deck
+    avg = []
+    for n in (8, 16, 32):
+        _, _, res, _ = mms_solve(dataclasses.replace(d0, nx=n, ny=n, nz=n))
+        avg.append(res["avg"])
+    assert avg[0] / avg[1] > 3.0 and avg[1] / avg[2] > 3.0, avg
+    assert avg[2] < AVG_LIMIT

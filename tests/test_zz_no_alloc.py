@@ -42,6 +42,9 @@ def test_noalloc_sweep_matches_context_sweep(d):
                                      torch.as_tensor(prob["mat"], device="cuda"))
     rng = np.random.default_rng(21)
     stream = torch.cuda.current_stream().cuda_stream
+    # set-up call (all arrays NULL): places the static array and the sweep's
+    # code on the device, so the sweeps below reserve no device memory
+    abi.check(lib.snap_sweep_noalloc(C.byref(cfg), None, None, None, stream))
     for call in range(2):
         q = rng.uniform(0.0, 1.0, size=(d.ng, d.cells, d.cmom))
         if d.cmom > 1:
@@ -49,9 +52,13 @@ def test_noalloc_sweep_matches_context_sweep(d):
         qtot = torch.as_tensor(q, device="cuda")
         want = snap.mini_kba_sweep(qtot, t_xs)
         got = torch.full_like(want, float("nan"))
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
         rc = lib.snap_sweep_noalloc(C.byref(cfg), qtot.data_ptr(), t_xs.data_ptr(),
                                     got.data_ptr(), stream)
         abi.check(rc)
+        torch.cuda.synchronize()
+        assert torch.cuda.mem_get_info()[0] == free_before, "the sweep reserved device memory"
         w, g = want.cpu().numpy(), got.cpu().numpy()
         scale = np.abs(w).reshape(-1, d.cmom).max(axis=0)
         err = (np.abs(g - w).reshape(-1, d.cmom).max(axis=0) / scale).max()
@@ -69,3 +76,14 @@ def test_noalloc_rejects_oversized_problem():
                                 dummy.data_ptr(), torch.cuda.current_stream().cuda_stream)
     assert rc == 2   # SNAP_ERR_UNSUPPORTED
     assert b"static limit" in lib.snap_last_error()
+
+
+def test_noalloc_rejects_partial_null_arrays():
+    lib = abi.load()
+    d = P.deck(1)
+    host = [np.ascontiguousarray(a) for a in P.quadrature(d.nang, d.nmom)]
+    cfg = config(d, host)
+    dummy = torch.zeros(1, dtype=torch.float64, device="cuda")
+    rc = lib.snap_sweep_noalloc(C.byref(cfg), dummy.data_ptr(), None, dummy.data_ptr(),
+                                torch.cuda.current_stream().cuda_stream)
+    assert rc == 1   # SNAP_ERR_BAD_ARG
