@@ -23,9 +23,16 @@ L2 flush is needed between steps.
   cpu_baseline  the reference's own CPU task bodies (oracle/_ref) on the host
           cores, bounded sample
 
---impl reference times the reference's CPU path alone (rank 0 only).
-Multi-GPU (torchrun): each rank owns a 32-group shard (weak scaling); the
-only exchange in a step is the convergence AND (NCCL all-reduce of one int).
+  same_config  deck 2' (deck 2 at nmom = 1) on the GPU against the reference's
+          own task bodies running the same step (the reference's CPU path
+          cannot run nmom > 1)
+
+--impl reference times the reference's CPU path alone (rank 0 only) on deck
+2', the same step.
+Multi-GPU (torchrun): each rank owns a 32-group shard of a 32*N-group deck
+(weak scaling); every step ANDs the inner tests over the ranks and every
+iitm-th step carries the per-outer exchange (NCCL all-gather of the flux
+moments, then each rank's outer source from all groups).
 """
 from __future__ import annotations
 
@@ -78,9 +85,10 @@ def deck2():
 
 
 def workload_config(d, precision="fp64"):
+    name = "deck 2" if d.nmom == 4 else f"deck 2' (deck 2 at nmom={d.nmom})"
     return {
-        "workload": "deck 2: 64^3 cells, 36 angles/octant, 32 groups, nmom=4 (16 moments), "
-                    "steady-state fixed source, fixup on",
+        "workload": f"{name}: {d.nx}^3 cells, {d.nang} angles/octant, {d.ng} groups, "
+                    f"nmom={d.nmom} ({d.cmom} moments), steady-state fixed source, fixup on",
         "cells": d.cells, "angles_per_octant": d.nang, "groups": d.ng, "nmom": d.nmom,
         "cmom": d.cmom, "precision": precision,
         "step": "one inner iteration: inner source + sweep of 8 octants x all groups + "
@@ -170,57 +178,102 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
-def cpu_reference_sample(d, inners: int):
-    """The reference's own CPU task bodies on deck 2's mesh, angles and groups
-    at nmom = 1 (its nmom > 1 sweep path dereferences an unbound flux-moment
-    accessor), all host threads, `inners` inner iterations."""
+def deck2_prime():
+    """Deck 2 at one moment (nmom = 1): the largest configuration of the
+    benchmark deck the reference's CPU path can run (its nmom > 1 sweep
+    dereferences an unbound flux-moment accessor, sweep.cc:312-317 against
+    :575-590)."""
+    from snap_b200 import problem as P
+    return P.deck(2, nmom=1) if GROUPS is None else P.deck(2, nmom=1, ng=GROUPS)
+
+
+def cpu_reference_sample(steps: int, warmup: int = 0):
+    """The reference's own CPU task bodies (oracle/_ref) on deck 2' running
+    exactly the GPU step: `steps` inner iterations (inner source, sweep,
+    inner test; group-parallel on every host thread, as the reference's
+    index launches run), after `warmup` untimed ones and one outer source."""
     from oracle.bindings import RefSnap
     from snap_b200 import problem as P
     if not RefSnap.available():
         return None
-    dd = P.Deck(**{**d.__dict__, "nmom": 1})
-    ref = RefSnap(dd)
-    prob = P.make_problem(dd)
+    d = deck2_prime()
+    prob = P.make_problem(d)
+    ref = RefSnap(d)
     threads = os.cpu_count() or 1
-    _, rec = ref.solve(prob, nthreads=threads, max_inners=inners)
-    grind = rec["seconds"] * 1e9 / (dd.units_per_sweep * rec["inner_total"])
+    if warmup:
+        ref.time_inner(prob, warmup, nthreads=threads)
+    r = ref.time_inner(prob, steps, nthreads=threads)
+    grind = r["seconds"] * 1e9 / (d.units_per_sweep * steps)
     return {"value": grind, "unit": UNIT, "cores": threads, "kind": "reference",
-            "sample": f"reference CPU task bodies (variant {rec['variant']}: "
-                      f"{['scalar', 'SSE', 'AVX'][rec['variant']]}), deck 2 mesh/angles/groups "
-                      f"at nmom=1, {rec['inner_total']} inner iterations incl. one outer source, "
-                      f"{threads} threads",
-            "sweep_only_ns": rec["sweep_seconds"] * 1e9 / (dd.units_per_sweep * rec["inner_total"])}
+            "sample": f"reference CPU task bodies (variant {r['variant']}: "
+                      f"{['scalar', 'SSE', 'AVX'][r['variant']]}), deck 2' (deck 2 at nmom=1), "
+                      f"{steps} inner iterations (inner source + sweep + inner test, "
+                      f"group-parallel), {threads} threads",
+            "sweep_only_ns": r["sweep_seconds"] * 1e9 / (d.units_per_sweep * steps),
+            "ms_per_step": r["seconds"] * 1e3 / steps}
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    d = deck2()
-    vals = []
-    sample = None
-    for i in range(args.warmup + args.steps):
-        s = cpu_reference_sample(d, 1)
-        if s is None:
-            print(json.dumps({"impl": "reference", "unavailable":
-                              "reference CPU build oracle/_ref/libsnapref.so not present"}))
-            return 0
-        if i >= args.warmup:
-            vals.append(s["value"])
-            sample = s
-    value = statistics.median(vals)
+    d = deck2_prime()
+    s = cpu_reference_sample(args.steps, args.warmup)
+    if s is None:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "reference CPU build oracle/_ref/libsnapref.so not present"}))
+        return 0
+    value = s["value"]
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": value * d.units_per_sweep / 1e6, "higher_is_better": False,
+        "ms_per_step": s["ms_per_step"], "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": workload_config(d, "fp64 (reference CPU at nmom=1)"),
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": sample["cores"],
-                         "kind": "reference", "sample": sample["sample"]},
+        "config": workload_config(d, "fp64"),
+        "note": "the reference's CPU path runs nmom = 1 only, so this arm times deck 2' (deck 2 "
+                "at nmom = 1, same mesh, angles and groups); the GPU arm's headline is deck 2 at "
+                "nmom = 4 and its same_config block times deck 2' on the GPU",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": s["cores"],
+                         "kind": "reference", "sample": s["sample"]},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
     return 0
+
+
+def gpu_inner_grind(d, steps, warmup, local, precision="fp64"):
+    """Device-resident inner iterations of deck d on one GPU: ms per step and
+    grind time."""
+    import torch
+
+    from snap_b200 import problem as P
+    from snap_b200.solver import Snap
+    snap = Snap(d, precision=precision, device=local)
+    prob = P.make_problem(d)
+    dp = snap.device_problem(prob)
+    t_xs = snap.expand_cross_section(dp["sigt"], dp["mat"])
+    if precision != "fp64":
+        t_xs = t_xs.float()
+    s_xs = snap.expand_scattering_cross_section(dp["slgg"], dp["mat"])
+    flux = torch.zeros(d.ng, d.cells, d.cmom, dtype=torch.float64, device="cuda")
+    q2 = snap.calc_outer_source(dp["qi"], dp["slgg"], dp["mat"], flux)
+    qtot = torch.empty(d.ng, d.cells, d.cmom, dtype=snap.sweep_dtype, device="cuda")
+    for _ in range(warmup):
+        snap.inner_iteration(s_xs, q2, t_xs, flux, qtot)
+    torch.cuda.synchronize()
+    snap.timing(reset=True)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        snap.inner_iteration(s_xs, q2, t_xs, flux, qtot)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    tm = snap.timing()
+    snap.close()
+    return {"ms_per_step": ms, "value": ms * 1e6 / d.units_per_sweep,
+            "sweep_ms": tm["sweep_ms"] / max(tm["sweep_calls"], 1)}
 
 
 MIXED_PRECISION = ("fp32 sweep (moment contractions on FP64 tensor cores); group-to-group "
@@ -376,13 +429,34 @@ def run_snap(args):
     q2grp = snap.calc_outer_source(dp["qi"], dp["slgg"], dp["mat"], flux)
     qtot = torch.empty(d.ng, d.cells, d.cmom, dtype=torch.float64, device="cuda")
 
-    def step():
-        conv = snap.inner_iteration(s_xs, q2grp, t_xs, flux, qtot)
-        if world > 1:   # global convergence = AND over the group shards
-            flag = torch.tensor([0 if conv else 1], dtype=torch.int32, device="cuda")
-            dist.all_reduce(flag)
-            conv = int(flag.item()) == 0
-        return conv
+    step_no = [0]
+    if world > 1:
+        # weak scaling: rank r owns groups 32r .. 32r+31 of a 32*world-group
+        # deck; every iitm-th step carries the per-outer exchange (all-gather
+        # of every group's flux moments over NCCL, then the outer source of
+        # this rank's groups from all of them), every step the AND of the
+        # inner tests
+        import dataclasses
+
+        from snap_b200.parallel import GpuShard, TorchComm
+        d_total = dataclasses.replace(d, ng=d.ng * world)
+        shard = GpuShard(d_total, P.make_problem(d_total), rank * d.ng, d.ng, device=local)
+        comm = TorchComm(dist)
+        counts = [d.ng] * world
+        snap.close()
+        snap = shard.snap
+        flux = shard.zero_flux()
+        q2_box = [shard.outer_source(comm.all_gather_groups(flux, counts))]
+
+        def step():
+            if step_no[0] % d.iitm == 0:
+                q2_box[0] = shard.outer_source(comm.all_gather_groups(flux, counts))
+            step_no[0] += 1
+            return comm.all_true(shard.inner_iteration(q2_box[0], flux), shard.device)
+    else:
+        def step():
+            step_no[0] += 1
+            return snap.inner_iteration(s_xs, q2grp, t_xs, flux, qtot)
 
     for _ in range(args.warmup):
         step()
@@ -554,9 +628,21 @@ def run_snap(args):
     if adjoint is not None:
         line["adjoint"] = adjoint
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cb = cpu_reference_sample(d, args.cpu_inners)
+        cb = cpu_reference_sample(args.cpu_inners)
         if cb is not None:
             line["cpu_baseline"] = cb
+            # the same configuration on both sides: deck 2' on the GPU, the
+            # same step as the reference's task bodies above
+            d1 = deck2_prime()
+            g1 = gpu_inner_grind(d1, args.steps, args.warmup, local)
+            line["same_config"] = {
+                "workload": workload_config(d1)["workload"],
+                "step": "one inner iteration (inner source + sweep + inner test), both sides",
+                "gpu_ns": g1["value"], "gpu_ms_per_step": g1["ms_per_step"],
+                "reference_ns": cb["value"], "reference_ms_per_step": cb["ms_per_step"],
+                "reference_over_gpu": cb["value"] / g1["value"],
+                "note": "the driver's reference arm times deck 2' (the reference cannot run "
+                        "nmom > 1); this block is the like-for-like ratio"}
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

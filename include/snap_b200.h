@@ -135,6 +135,20 @@ int snap_calc_inner_source(snap_ctx *ctx, const double *s_xs, const double *q2gr
  * FP64 context: qtot/t_xs/flux double.  FP32 context: float. */
 int snap_sweep(snap_ctx *ctx, const void *qtot, const void *t_xs, void *flux, void *stream);
 
+/* The time-dependent sweep of all 8 octants and groups (the MiniKBATask
+ * body with its time-flux and MMS regions, sweep.cc:354-591): as snap_sweep
+ * (flux zeroed first) with vdelt[g] * psi_t_in added to each angle's
+ * diamond-difference numerator and vdelt[g] to its denominator, the outgoing
+ * time face psi_t_out = 2 pc - psi_t_in (a fourth face of the fixup, with
+ * its own flag), and qim added to the angular source when not NULL; groups
+ * with vdelt == 0 sweep as in steady state.  vdelt [ng]; psi_t_in,
+ * psi_t_out and qim [octant][g][c][nang]; all device, FP64 contexts.  Runs
+ * the general sweep kernel.  Replaces run_gpu_sweep with time dependence
+ * (gpu_sweep.cu:738-1393). */
+int snap_sweep_td(snap_ctx *ctx, const double *qtot, const double *t_xs, const double *vdelt,
+                  const double *psi_t_in, double *psi_t_out, const double *qim, double *flux,
+                  void *stream);
+
 /* converged = every scalar flux satisfies |flux/prev - 1| <= epsi (or
  * |flux| <= epsi where |prev| < 1e-12).  kind 0: inner test (epsi as given);
  * kind 1: outer test, which the caller runs with 100*epsi and only when the

@@ -84,6 +84,15 @@ struct snap_ctx {
   double *d_vdelt0 = nullptr;   // [G] zeros: steady-state vdelt
   double *d_vdelt = nullptr;    // [G] vdelt of the current time-dependent solve
   std::vector<double> h_vdelt;
+  // adjoint with group batches: the forward state of `state_groups` groups at
+  // a time, recorded again for every batch of every adjoint iteration; work
+  // items of a batch of g groups in batch_tables[g]
+  int state_groups = 0;
+  struct BatchTables {
+    int n_items = 0;
+    int *table = nullptr, *index = nullptr;
+  };
+  std::vector<BatchTables> batch_tables;
   // solve arrays, kept between snap_transport_solve calls (first call allocates)
   void *d_solve = nullptr;
   double *s_txs64 = nullptr, *s_sxs = nullptr, *s_q2 = nullptr, *s_fpo = nullptr;
@@ -131,6 +140,10 @@ void free_ctx(snap_ctx *c) {
   cudaFree(c->d_vdelt0);
   cudaFree(c->d_vdelt);
   cudaFree(c->d_solve);
+  for (auto &b : c->batch_tables) {
+    cudaFree(b.table);
+    cudaFree(b.index);
+  }
   if (c->h_ctrl) cudaFreeHost(c->h_ctrl);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
@@ -283,25 +296,31 @@ void build_items(int P, int G, int tx_n, int ty_n, std::vector<int> &table,
 // With atomic_flux (forward mode only), every octant adds its moments into
 // that FP64 flux [G][C][cmom] instead of writing its slot.
 int sweep_launches(snap_ctx *c, const void *qtot, const void *t_xs, cudaStream_t st,
-                   int mode = 0, void *sbar = nullptr, double *atomic_flux = nullptr) {
+                   int mode = 0, void *sbar = nullptr, double *atomic_flux = nullptr,
+                   int g0 = 0, int gn = 0) {
+  // gn > 0: only groups g0 .. g0+gn-1 (qtot and t_xs hold every group; the
+  // slots, the recorded state and sbar hold the batch)
+  const bool batch = gn > 0 && gn < c->cfg.ng;
+  if (batch && ((int)c->batch_tables.size() <= gn || !c->batch_tables[gn].table))
+    return fail(SNAP_ERR_BAD_ARG, "no work items for this group batch");
   SweepParams p{};
   p.nx = c->cfg.nx;
   p.ny = c->cfg.ny;
   p.nz = c->cfg.nz;
   p.M = c->M;
   p.A = c->A;
-  p.G = c->cfg.ng;
+  p.G = batch ? gn : c->cfg.ng;
   p.tiles_x = c->tiles_x;
   p.tiles_y = c->tiles_y;
-  p.n_items = c->n_items;
+  p.n_items = batch ? c->batch_tables[gn].n_items : c->n_items;
   p.fixup = c->cfg.fixup;
   p.timeout_ns = c->timeout_ns;
   p.withhold_item1 = mode == 2 ? 0 : c->withhold_item1;
   c->withhold_item1 = 0;   // one launch only
-  p.item_table = c->d_item_table;
-  p.item_index = c->d_item_index;
-  p.qtot = qtot;
-  p.t_xs = t_xs;
+  p.item_table = batch ? c->batch_tables[gn].table : c->d_item_table;
+  p.item_index = batch ? c->batch_tables[gn].index : c->d_item_index;
+  p.qtot = (const char *)qtot + (size_t)g0 * c->C * c->M * c->wsize;
+  p.t_xs = (const char *)t_xs + (size_t)g0 * c->C * c->wsize;
   if (!atomic_flux && !c->d_slots) {
     if (cudaMalloc(&c->d_slots, c->slots_bytes) != cudaSuccess) {
       cudaGetLastError();
@@ -340,8 +359,9 @@ int sweep_launches(snap_ctx *c, const void *qtot, const void *t_xs, cudaStream_t
         blocks < 1)
       return fail(SNAP_ERR_UNSUPPORTED, "no adjoint kernel for this shape (8x4 tiles only)");
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-    grid = std::min(blocks * sms, c->n_items);
+    grid = std::min(blocks * sms, p.n_items);
   }
+  if (batch) grid = std::min(grid, p.n_items);
   for (int L = 0; L < 8 / c->P; ++L) {
     p.o_base = L * c->P;
     p.accumulate = L > 0;
@@ -801,6 +821,24 @@ int snap_sweep(snap_ctx *c, const void *qtot, const void *t_xs, void *flux, void
   return rc;
 }
 
+int snap_sweep_td(snap_ctx *c, const double *qtot, const double *t_xs, const double *vdelt,
+                  const double *psi_t_in, double *psi_t_out, const double *qim, double *flux,
+                  void *stream) {
+  if (!c || !qtot || !t_xs || !flux || !vdelt || !psi_t_in || !psi_t_out)
+    return fail(SNAP_ERR_BAD_ARG, "null argument");
+  if (c->fp32) return fail(SNAP_ERR_UNSUPPORTED, "time-dependent sweeps run in FP64 contexts");
+  cudaStream_t st = (cudaStream_t)stream;
+  SNAP_CUDA(cudaMemsetAsync(c->error(), 0, 2 * sizeof(int), st));
+  SNAP_CUDA(cudaMemsetAsync(flux, 0, sizeof(double) * c->cfg.ng * c->C * c->M, st));
+  SNAP_CUDA(cudaEventRecord(c->sw0, st));
+  int rc = wide_sweep(c, qtot, t_xs, flux, vdelt, psi_t_in, psi_t_out, qim, st);
+  if (rc) return rc;
+  SNAP_CUDA(cudaEventRecord(c->sw1, st));
+  rc = read_ctrl(c, st, nullptr);
+  if (rc == SNAP_OK) account_sweep(c);
+  return rc;
+}
+
 int snap_inner_iteration(snap_ctx *c, const double *s_xs, const double *q2grp, const void *t_xs,
                          double *flux, void *qtot, double epsi, int *converged, void *stream) {
   if (!c || !s_xs || !q2grp || !t_xs || !flux || !qtot || !converged)
@@ -1195,9 +1233,32 @@ int snap_transport_solve_td(snap_ctx *c, const int32_t *mat, const double *qi, c
 
 namespace {
 
-int ensure_state(snap_ctx *c) {
-  if (c->d_pc_store) return SNAP_OK;
-  const size_t n = (size_t)8 * c->cfg.ng * c->C * c->AP;
+// Work items of a batch of gn groups (same order rules as build_items).
+int ensure_batch_tables(snap_ctx *c, int gn) {
+  if ((int)c->batch_tables.size() <= gn) c->batch_tables.resize(gn + 1);
+  auto &b = c->batch_tables[gn];
+  if (b.table) return SNAP_OK;
+  std::vector<int> table, index;
+  build_items(c->P, gn, c->tiles_x, c->tiles_y, table, index);
+  int rc;
+  if ((rc = upload((void **)&b.table, table)) || (rc = upload((void **)&b.index, index))) return rc;
+  b.n_items = (int)table.size();
+  return SNAP_OK;
+}
+
+// Forward state for the adjoint of `groups` groups at a time.
+int ensure_state(snap_ctx *c, int groups = 0) {
+  if (groups <= 0) groups = c->cfg.ng;
+  if (c->d_pc_store && c->state_groups >= groups) return SNAP_OK;
+  if (c->d_pc_store) {
+    cudaFree(c->d_pc_store);
+    cudaFree(c->d_flag_store);
+    c->scratch_bytes -= (size_t)8 * c->state_groups * c->C * c->AP * (c->wsize + 1);
+    c->d_pc_store = nullptr;
+    c->d_flag_store = nullptr;
+    c->state_groups = 0;
+  }
+  const size_t n = (size_t)8 * groups * c->C * c->AP;
   if (cudaMalloc(&c->d_pc_store, n * c->wsize) != cudaSuccess ||
       cudaMalloc((void **)&c->d_flag_store, n) != cudaSuccess) {
     cudaGetLastError();
@@ -1206,6 +1267,7 @@ int ensure_state(snap_ctx *c) {
     return fail(SNAP_ERR_OOM, "cannot allocate the forward-state store for the adjoint");
   }
   c->scratch_bytes += n * (c->wsize + 1);
+  c->state_groups = groups;
   return SNAP_OK;
 }
 
@@ -1221,22 +1283,41 @@ int ensure_sbar(snap_ctx *c) {
 }
 
 int adjoint_sweep_impl(snap_ctx *c, const void *phi_bar, const void *t_xs, double *qtot_bar,
-                       double *sigt_bar, cudaStream_t st) {
-  if ((sigt_bar || c->cfg.fixup) && !c->state_recorded)
+                       double *sigt_bar, cudaStream_t st, int g0 = 0, int gn = 0) {
+  const int groups = gn > 0 ? gn : c->cfg.ng;
+  if ((sigt_bar || c->cfg.fixup) && (!c->state_recorded || c->state_groups < groups))
     return fail(SNAP_ERR_BAD_ARG, "record the forward state (snap_record_forward) first");
   int rc;
   if (sigt_bar && (rc = ensure_sbar(c))) return rc;
   SNAP_CUDA(cudaEventRecord(c->sw0, st));
-  rc = sweep_launches(c, phi_bar, t_xs, st, 2, sigt_bar ? c->d_sbar_slots : nullptr);
+  rc = sweep_launches(c, phi_bar, t_xs, st, 2, sigt_bar ? c->d_sbar_slots : nullptr, nullptr, g0,
+                      gn);
   if (rc) return rc;
   SNAP_CUDA(cudaEventRecord(c->sw1, st));
-  SNAP_CUDA(k_reduce_slots(c->d_slots, c->P, c->fp32, qtot_bar, 0, nullptr, c->cfg.ng, c->M, c->C,
-                           0, 0.0, nullptr, st));
+  SNAP_CUDA(k_reduce_slots(c->d_slots, c->P, c->fp32, qtot_bar + (size_t)g0 * c->C * c->M, 0,
+                           nullptr, groups, c->M, c->C, 0, 0.0, nullptr, st));
   ++c->launches;
   if (sigt_bar) {
-    SNAP_CUDA(k_reduce_slots(c->d_sbar_slots, c->P, c->fp32, sigt_bar, 0, nullptr, c->cfg.ng, 1,
-                             c->C, 0, 0.0, nullptr, st));
+    SNAP_CUDA(k_reduce_slots(c->d_sbar_slots, c->P, c->fp32, sigt_bar + (size_t)g0 * c->C, 0,
+                             nullptr, groups, 1, c->C, 0, 0.0, nullptr, st));
     ++c->launches;
+  }
+  return SNAP_OK;
+}
+
+// One application of M^T L^-T D^T to every group (qtot_bar from phi_bar),
+// with the forward state recorded from `qtot` batch by batch when the
+// context holds the state of fewer groups than it sweeps.
+int adjoint_apply(snap_ctx *c, const void *phi_bar, const void *t_xs, const void *qtot,
+                  double *qtot_bar, double *sigt_bar, cudaStream_t st, int batch) {
+  const int G = c->cfg.ng;
+  if (batch >= G) return adjoint_sweep_impl(c, phi_bar, t_xs, qtot_bar, sigt_bar, st);
+  for (int g0 = 0; g0 < G; g0 += batch) {
+    const int gn = std::min(batch, G - g0);
+    int rc = sweep_launches(c, qtot, t_xs, st, 1, nullptr, nullptr, g0, gn);
+    if (rc) return rc;
+    rc = adjoint_sweep_impl(c, phi_bar, t_xs, qtot_bar, sigt_bar, st, g0, gn);
+    if (rc) return rc;
   }
   return SNAP_OK;
 }
@@ -1311,7 +1392,24 @@ int snap_adjoint_solve(snap_ctx *c, const int32_t *mat, const double *qi, const 
     cleanup();
     return fail(SNAP_ERR_OOM, "cannot allocate adjoint solve arrays");
   }
-  int rc = ensure_state(c);
+  // forward state of `batch` groups at a time: all groups when it fits in
+  // 70 % of the free memory (recorded once), else batches recorded again
+  // from the converged flux moments for every adjoint iteration
+  int batch = G;
+  {
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    const size_t per_group = (size_t)8 * C * c->AP * (c->wsize + 1);
+    const size_t held = c->d_pc_store ? (size_t)c->state_groups * per_group : 0;
+    const size_t avail = (size_t)(0.7 * (double)(free_b + held));
+    batch = (int)std::max<size_t>(1, std::min<size_t>((size_t)G, avail / per_group));
+    if (const char *e = getenv("SNAP_B200_ADJOINT_GROUPS")) batch = std::max(1, std::min(G, atoi(e)));
+  }
+  int rc = ensure_state(c, batch);
+  if (!rc && batch < G) {
+    rc = ensure_batch_tables(c, batch);
+    if (!rc && G % batch) rc = ensure_batch_tables(c, G % batch);
+  }
   if (rc) {
     cleanup();
     return rc;
@@ -1338,9 +1436,12 @@ int snap_adjoint_solve(snap_ctx *c, const int32_t *mat, const double *qi, const 
     ASTEP(k_outer_source(qi, slgg, mat, flux, q2grp, G, c->cfg.nmat, nmom, M, C, st));
     ASTEP(k_inner_source(s_xs, q2grp, flux, qtot, c->fp32, G, nmom, M, C, st));
     c->launches += c->fp32 ? 4 : 3;
-    // forward sweep recording the cell-average fluxes and fixup flags
-    rc = sweep_launches(c, qtot, c->fp32 ? t_xs_sw : t_xs64, st, 1);
-    if (rc) goto adone;
+    // forward sweep recording the cell-average fluxes and fixup flags (with
+    // batches: recorded inside every adjoint application)
+    if (batch >= G) {
+      rc = sweep_launches(c, qtot, c->fp32 ? t_xs_sw : t_xs64, st, 1);
+      if (rc) goto adone;
+    }
     c->state_recorded = true;
     // adjoint source iteration: phi_bar = r + S^T M^T L^-T D^T phi_bar,
     // converged when max|change| <= epsi * max|phi_bar| (the adjoint spans
@@ -1355,7 +1456,7 @@ int snap_adjoint_solve(snap_ctx *c, const int32_t *mat, const double *qi, const 
         ++c->launches;
         src = pb_sw;
       }
-      rc = adjoint_sweep_impl(c, src, c->fp32 ? t_xs_sw : t_xs64, qbar, nullptr, st);
+      rc = adjoint_apply(c, src, c->fp32 ? t_xs_sw : t_xs64, qtot, qbar, nullptr, st, batch);
       if (rc) goto adone;
       ASTEP(k_adjoint_scatter(response, slgg, mat, qbar, pb2, G, c->cfg.nmat, nmom, M, C, st));
       ASTEP(cudaMemsetAsync(d_norm, 0, 2 * sizeof(unsigned long long), st));
@@ -1385,7 +1486,7 @@ int snap_adjoint_solve(snap_ctx *c, const int32_t *mat, const double *qi, const 
         ++c->launches;
         src = pb_sw;
       }
-      rc = adjoint_sweep_impl(c, src, c->fp32 ? t_xs_sw : t_xs64, qbar, grad_sigt, st);
+      rc = adjoint_apply(c, src, c->fp32 ? t_xs_sw : t_xs64, qtot, qbar, grad_sigt, st, batch);
       if (rc) goto adone;
     }
     ASTEP(k_moment0(qbar, grad_qi, M, n, st));

@@ -82,6 +82,7 @@ SIGNATURES = {
                            C.POINTER(SnapSolveInfo), _vp],
     "snap_sweep_noalloc": [C.POINTER(SnapConfig), _vp, _vp, _vp, _vp],
     "snap_inject_stall": [_vp, C.c_int],
+    "snap_sweep_td": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "snap_mms_init": [_vp, _vp, _vp, _vp, C.c_double, C.c_double, C.c_double, C.c_int,
                       C.c_double, C.c_double, _vp, _vp, _vp, _vp],
     "snap_mms_compare": [_vp, _vp, _vp, _vp, _vp],

