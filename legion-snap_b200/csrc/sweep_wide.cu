@@ -74,6 +74,30 @@ __global__ void __launch_bounds__(MAX_THREADS) wide_sweep_kernel(const WideParam
     xin[k] = 0.0;
   }
 
+  // The inputs of a cell (sigma_t, the scalar source, and per angle the MMS
+  // source, the time-edge flux and the incoming y and z faces) are loaded one
+  // cell ahead, while the cell before is computed.  The faces a cell reads
+  // were written by this thread at an earlier cell, except when the mesh is
+  // one cell wide (nx = 1: the y face of the next pencil is this cell's; nx
+  // = ny = 1: so is the z face), where they are forwarded from registers.
+  double n_sig = 0.0, n_q0 = 0.0;
+  double n_qim[APT], n_iy[APT], n_iz[APT], n_it[APT];
+  auto load_cell = [&](int xx, int yy, int zz) {
+    const int x = sx ? xx : nx - 1 - xx, y = sy ? yy : ny - 1 - yy, z = sz ? zz : nz - 1 - zz;
+    const long long c = ((long long)z * ny + y) * nx + x;
+    n_sig = __ldg(tg + c);
+    n_q0 = __ldg(qg + c * M);
+#pragma unroll
+    for (int k = 0; k < APT; ++k) {
+      const int a = on[k] ? ang[k] : 0;
+      n_qim[k] = (p.qim && on[k]) ? p.qim[(field + c) * A + a] : 0.0;
+      n_it[k] = (tt && on[k]) ? p.tf_in[(field + c) * A + a] : 0.0;
+      n_iy[k] = (yy == 0 || !on[k]) ? 0.0 : ypen[(size_t)xx * A + a];
+      n_iz[k] = (zz == 0 || !on[k]) ? 0.0 : zpl[((size_t)yy * nx + xx) * A + a];
+    }
+  };
+  load_cell(0, 0, 0);
+
   for (int zz = 0; zz < nz; ++zz) {
     const int z = sz ? zz : nz - 1 - zz;
     for (int yy = 0; yy < ny; ++yy) {
@@ -82,9 +106,22 @@ __global__ void __launch_bounds__(MAX_THREADS) wide_sweep_kernel(const WideParam
         const int x = sx ? xx : nx - 1 - xx;
         const long long c = ((long long)z * ny + y) * nx + x;
         const double *q = qg + c * M;
-        const double sig = __ldg(tg + c);
-        const double q0 = __ldg(q);
-        double pc[APT], psi[APT], iy[APT], iz[APT], it[APT];
+        const double sig = n_sig;
+        const double q0 = n_q0;
+        double pc[APT], psi[APT], iy[APT], iz[APT], it[APT], qm[APT];
+#pragma unroll
+        for (int k = 0; k < APT; ++k) {
+          iy[k] = n_iy[k];
+          iz[k] = n_iz[k];
+          it[k] = n_it[k];
+          qm[k] = n_qim[k];
+        }
+        // the next cell's inputs
+        const bool more = xx + 1 < nx || yy + 1 < ny || zz + 1 < nz;
+        const int nxx = xx + 1 < nx ? xx + 1 : 0;
+        const int nyy = xx + 1 < nx ? yy : (yy + 1 < ny ? yy + 1 : 0);
+        const int nzz = (xx + 1 < nx || yy + 1 < ny) ? zz : zz + 1;
+        if (more) load_cell(nxx, nyy, nzz);
         bool neg = false;
 #pragma unroll
         for (int k = 0; k < APT; ++k) {
@@ -92,13 +129,9 @@ __global__ void __launch_bounds__(MAX_THREADS) wide_sweep_kernel(const WideParam
           // angular source (sweep.cc:354-375)
           double s = q0;
           for (int m = 1; m < M; ++m) s += ec[(size_t)m * A + a] * __ldg(q + m);
-          if (p.qim && on[k]) s += p.qim[(field + c) * A + a];
+          if (p.qim && on[k]) s += qm[k];
           psi[k] = s;
           if (xx == 0) xin[k] = 0.0;   // vacuum x boundary (single chunk)
-          const size_t yo = (size_t)xx * A + a, zo = ((size_t)yy * nx + xx) * A + a;
-          iy[k] = (yy == 0 || !on[k]) ? 0.0 : ypen[yo];
-          iz[k] = (zz == 0 || !on[k]) ? 0.0 : zpl[zo];
-          it[k] = (tt && on[k]) ? p.tf_in[(field + c) * A + a] : 0.0;
           // diamond difference with the geometry parameter (expxs.cc:384-385,
           // sweep.cc:377-423)
           double v = s + xin[k] * cx[k];
@@ -161,10 +194,14 @@ __global__ void __launch_bounds__(MAX_THREADS) wide_sweep_kernel(const WideParam
           const int a = ang[k];
           const double v2 = 2.0 * pc[k];
           xin[k] = (v2 - xin[k]) * hx[k];
-          ypen[(size_t)xx * A + a] = (v2 - iy[k]) * hy[k];
-          zpl[((size_t)yy * nx + xx) * A + a] = (v2 - iz[k]) * hz[k];
+          const double oy = (v2 - iy[k]) * hy[k], oz = (v2 - iz[k]) * hz[k];
+          ypen[(size_t)xx * A + a] = oy;
+          zpl[((size_t)yy * nx + xx) * A + a] = oz;
           if (tt) p.tf_out[(field + c) * A + a] = (v2 - it[k]) * ht[k];
           part0 += wt[k] * pc[k];
+          // one-cell-wide meshes: the next cell's face is this cell's output
+          if (nx == 1 && nyy > 0 && more) n_iy[k] = oy;
+          if (nx == 1 && ny == 1 && nzz > 0 && more) n_iz[k] = oz;
         }
         // per-warp moment partials of this cell into shared memory
         double *red = s_red + ((size_t)warp * nx + xx) * M;
