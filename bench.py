@@ -26,6 +26,9 @@ L2 flush is needed between steps.
   same_config  deck 2' (deck 2 at nmom = 1) on the GPU against the reference's
           own task bodies running the same step (the reference's CPU path
           cannot run nmom > 1)
+  reference_decks  the reference's own time-dependent performance decks
+          (input/*_4K_1x1x1.in) solved on the GPU, beside a bounded sample of
+          the reference's task bodies on the same decks
 
 --impl reference times the reference's CPU path alone (rank 0 only) on deck
 2', the same step.
@@ -71,6 +74,10 @@ def parse():
     ap.add_argument("--no-memory-deck", action="store_true",
                     help="skip the FP32 forward solve on the 192^3, 64-group, nmom 3 deck")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint leg")
+    ap.add_argument("--no-decks", action="store_true",
+                    help="skip the reference's own time-dependent decks")
+    ap.add_argument("--decks", default="tiny_4K_1x1x1.in,small_4K_1x1x1.in,medium_4K_1x1x1.in,"
+                                       "large_4K_1x1x1.in,huge_4K_1x1x1.in")
     ap.add_argument("--groups", type=int, default=None,
                     help="override deck 2's 32 groups (small cases for profiling only)")
     return ap.parse_args()
@@ -372,7 +379,9 @@ def memory_pressure_deck(local):
     from snap_b200.solver import Snap
     d = P.deck(5)
     res = {"deck": "192^3 cells, 48 angles/octant, 64 groups, nmom=3 (9 moments), random 50% "
-                   "material mix in the central 96^3 block, fixup on, FP32 sweep",
+                   "material mix in the central 96^3 block, fixup on, FP32 sweep; adjoint of a "
+                   "4^3 far-corner detector (weights 1/g), forward state recorded in group "
+                   "batches from the converged moments",
            "units_per_sweep": d.units_per_sweep}
     old = os.environ.get("SNAP_B200_OCTANTS_PER_LAUNCH")
     os.environ["SNAP_B200_OCTANTS_PER_LAUNCH"] = "1"
@@ -390,6 +399,27 @@ def memory_pressure_deck(local):
                     "scalar_flux_positive_finite": bool(torch.isfinite(flux).all()
                                                         and (flux[..., 0] > 0).all()),
                     "device_gb_in_use_after_solve": (total - free) / 1e9})
+        # the adjoint of the same deck on the same context (FP32 adjoint
+        # vectors in the context's solve arrays, state in group batches)
+        try:
+            r = torch.zeros(d.ng, d.nz, d.ny, d.nx, dtype=torch.float64, device="cuda")
+            r[:, -4:, -4:, -4:] = (1.0 / torch.arange(1, d.ng + 1, dtype=torch.float64,
+                                                      device="cuda"))[:, None, None, None]
+            r = r.reshape(d.ng, d.cells)
+            t_xs = snap.expand_cross_section(dp["sigt"], dp["mat"])
+            torch.cuda.empty_cache()
+            g = snap.adjoint_solve(dp, t_xs, flux, r, epsi=1e-5, with_sxs=False)
+            free, total = torch.cuda.mem_get_info()
+            res["adjoint"] = {"ms": g["total_ms"], "iterations": g["iterations"],
+                              "converged": g["converged"],
+                              "adjoint_over_forward": g["total_ms"] / rec["total_ms"],
+                              "grad_sigt_finite": bool(torch.isfinite(g["grad_sigt"]).all()),
+                              "grad_qi_finite": bool(torch.isfinite(g["grad_qi"]).all()),
+                              "device_gb_in_use": (total - free) / 1e9,
+                              "scratch_gb": snap.scratch_bytes / 1e9}
+            del g, r, t_xs
+        except Exception as e:   # report, do not lose the main bench line
+            res["adjoint"] = {"error": f"{type(e).__name__}: {e}"}
         del flux, dp
         snap.close()
         del snap
@@ -402,6 +432,49 @@ def memory_pressure_deck(local):
         else:
             os.environ["SNAP_B200_OCTANTS_PER_LAUNCH"] = old
     return res
+
+
+def reference_decks(names, local, cpu: bool):
+    """The reference's own performance decks (input/*_1x1x1.in: time
+    dependent, 10 steps, 16 x 16 x 16 cells, 32 to 1024 angles, 16 to 96
+    groups), solved whole on the GPU (second of two solves timed) and, when
+    `cpu`, a bounded sample of the reference's task bodies on the same deck
+    (2 inner iterations incl. one outer source, all host threads): time per
+    inner iteration on both sides."""
+    import torch
+
+    from snap_b200 import input_deck as D
+    from snap_b200 import problem as P
+    from snap_b200.solver import Snap
+    out = {}
+    for name in names:
+        try:
+            d = D.parse_deck(ROOT / "tests" / "decks" / name).deck
+            prob = P.make_problem(d)
+            snap = Snap(d, device=local)
+            dp = snap.device_problem(prob)
+            snap.transport_solve(dp)
+            flux, rec = snap.transport_solve(dp)
+            snap.close()
+            del snap, flux, dp
+            torch.cuda.empty_cache()
+            r = {"angles": d.nang, "groups": d.ng, "cells": d.cells, "steps": d.nsteps,
+                 "gpu_solve_ms": rec["total_ms"], "inner_iterations": rec["inner_total"],
+                 "gpu_ms_per_inner": rec["total_ms"] / rec["inner_total"],
+                 "gpu_sweep_ps_per_unit": rec["sweep_ms"] / rec["inner_total"] * 1e9
+                                          / d.units_per_sweep}
+            if cpu:
+                from oracle.bindings import RefSnap
+                if RefSnap.available():
+                    _, rr = RefSnap(d).solve(prob, nthreads=os.cpu_count() or 1, max_inners=2)
+                    r["reference_cpu_ms_per_inner"] = rr["seconds"] * 1e3 / rr["inner_total"]
+                    r["reference_cpu_threads"] = os.cpu_count() or 1
+                    r["reference_over_gpu_per_inner"] = (r["reference_cpu_ms_per_inner"]
+                                                         / r["gpu_ms_per_inner"])
+            out[name] = r
+        except Exception as e:   # report, do not lose the main bench line
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+    return out
 
 
 def run_snap(args):
@@ -569,8 +642,6 @@ def run_snap(args):
         del snap32, qtot32, flux32, q2grp32
         if not args.no_mixed_large:
             mixed["large_deck"] = mixed_large_deck(local)
-        if not args.no_memory_deck:
-            mixed["memory_pressure_deck"] = memory_pressure_deck(local)
 
     # adjoint cost on the adjoint deck (32^3, 24 angles, 16 groups, nmom 2,
     # per-cell sigma_t +-10 %): one converged forward solve and one converged
@@ -643,11 +714,23 @@ def run_snap(args):
                 "reference_over_gpu": cb["value"] / g1["value"],
                 "note": "the driver's reference arm times deck 2' (the reference cannot run "
                         "nmom > 1); this block is the like-for-like ratio"}
+    if rank == 0 and world == 1 and not args.no_decks:
+        line["reference_decks"] = reference_decks(
+            [x for x in args.decks.split(",") if x], local, not args.no_cpu_baseline)
+    # the 192^3 deck needs nearly all of the device: run it last, after the
+    # other legs' contexts and tensors are released
+    snap.close()
+    if mixed is not None and not args.no_memory_deck:
+        del flux, qtot, q2grp, t_xs, s_xs, dp
+        if args.e2e_solves > 0:
+            del out, dev
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        mixed["memory_pressure_deck"] = memory_pressure_deck(local)
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
-    snap.close()
     return 0
 
 

@@ -273,16 +273,23 @@ int snap_transport_solve_td(snap_ctx *ctx, const int32_t *mat, const double *qi,
  * ref_flux / v_g and ref_flux scaled to tf - dt/2, the solution at the middle
  * of the last step (mms.cc:387-418); then pass qim to snap_transport_solve_td
  * with qim_time_scaled = 1.  sigt [G][nmat] and slgg as for the solve.
- * Replaces MMSInitFlux, MMSInitSource and MMSInitTimeDependent
- * (snap.cc:373-388).  Synchronises `stream`. */
+ * chunk_cells = cells per spatial chunk along x, y, z (the deck's nx/ichunk,
+ * ny/npey, nz/npez; NULL: one chunk): each chunk's cell edges start at its
+ * first cell times that axis's spacing and then step by dx, as the
+ * reference's per-chunk tasks compute them, which differs from one chunk
+ * only when the spacings differ.  Replaces MMSInitFlux, MMSInitSource and
+ * MMSInitTimeDependent (snap.cc:373-388).  Synchronises `stream`. */
 int snap_mms_init(snap_ctx *ctx, const int32_t *mat, const double *sigt, const double *slgg,
-                  double lx, double ly, double lz, int timedep, double tf, double dt,
-                  double *ref_flux, double *qim, double *qi, void *stream);
+                  double lx, double ly, double lz, const int *chunk_cells, int timedep,
+                  double tf, double dt, double *ref_flux, double *qim, double *qi,
+                  void *stream);
 
 /* out[0], out[1], out[2] = max, min and sum over cells and groups of
  * |flux/ref - 1| (|flux| where ref < 1e-12); flux holds cmom moments per
  * cell (the scalar one is compared).  The reference fails the check when the
- * max exceeds 0.1 or the sum / (cells * groups) exceeds 1e-3 (snap.cc:542-560).
+ * max exceeds 0.1 or the sum / (cells * chunks * groups) exceeds 1e-3
+ * (snap.cc:542-560; its divisor multiplies the global cell count by the
+ * number of chunks).
  * Replaces MMSCompare (mms.cc:498-545).  Synchronises `stream`. */
 int snap_mms_compare(snap_ctx *ctx, const double *flux, const double *ref_flux, double *out,
                      void *stream);

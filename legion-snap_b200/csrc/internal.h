@@ -79,6 +79,7 @@ cudaError_t launch_sweep_wide(const WideParams &p, int n_blocks, cudaStream_t st
 // The manufactured-solution check (mms.cu).
 struct MmsGeometry {
   int nx, ny, nz, A, G, nmat;
+  int chunk[3];            // cells per spatial chunk along x, y, z
   double lx, ly, lz;
   int timedep;
   double tf, dt;
@@ -180,6 +181,16 @@ cudaError_t k_scale(double *x, double f, size_t n, cudaStream_t st);
 cudaError_t k_adjoint_scatter(const double *r, const double *slgg, const int32_t *mat,
                               const double *qbar, double *phi_bar, int G, int nmat, int nmom,
                               int M, long long C, cudaStream_t st);
+// phi_bar = r + S^T qbar in place (qbar and phi_bar float when fp32, else
+// double), norm[0] = max |change|, norm[1] = max |phi_bar| (bit patterns;
+// norm must start at zero)
+cudaError_t k_adjoint_update(const double *r, const double *slgg, const int32_t *mat,
+                             const void *qbar, void *phib, int fp32, unsigned long long *norm,
+                             int G, int nmat, int nmom, int M, long long C, cudaStream_t st);
+cudaError_t k_grad_sxs_any(const void *qbar, int fp32, const double *flux, double *grad, int G,
+                           int nmom, int M, long long C, cudaStream_t st);
+cudaError_t k_moment0_any(const void *in, int fp32, double *out, int M, long long n,
+                          cudaStream_t st);
 // grad[g][c][l] = sum_{k in band l} qbar[g][c][k] flux[g][c][k]
 cudaError_t k_grad_sxs(const double *qbar, const double *flux, double *grad, int G, int nmom,
                        int M, long long C, cudaStream_t st);

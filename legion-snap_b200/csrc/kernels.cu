@@ -247,7 +247,57 @@ __global__ void adjoint_scatter_kernel(const double *__restrict__ r, const doubl
   }
 }
 
-__global__ void grad_sxs_kernel(const double *__restrict__ qbar, const double *__restrict__ flux,
+// The adjoint source update in place: phib = r + S^T qbar (as
+// adjoint_scatter_kernel), with max |new - old| and max |new| accumulated in
+// norm[0..1] as bit patterns of non-negative doubles (NaN differences count
+// as infinite).  QT/PT: the types of qbar and phib (the sweep precision).
+template <int CELLS, typename QT, typename PT>
+__global__ void adjoint_update_kernel(const double *__restrict__ r, const double *__restrict__ slgg,
+                                      const int32_t *__restrict__ mat,
+                                      const QT *__restrict__ qbar, PT *__restrict__ phib,
+                                      unsigned long long *__restrict__ norm, int G, int nmat,
+                                      int nmom, int M, long long C) {
+  extern __shared__ double sq[];   // [G][CELLS][M]
+  double md = 0.0, ma = 0.0;
+  const long long ntiles = (C + CELLS - 1) / CELLS;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const long long c0 = tile * CELLS;
+    const int nc = (int)min((long long)CELLS, C - c0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < G * CELLS * M; i += blockDim.x) {
+      const int m = i % M, cc = (i / M) % CELLS, g = i / (M * CELLS);
+      sq[i] = cc < nc ? (double)qbar[((size_t)g * C + c0 + cc) * M + m] : 0.0;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < G * CELLS * M; i += blockDim.x) {
+      const int m = i % M, cc = (i / M) % CELLS, g2 = i / (M * CELLS);
+      if (cc >= nc) continue;
+      const long long c = c0 + cc;
+      const int l = band_of(m), mt = mat[c] - 1;
+      double acc = (m == 0) ? r[(size_t)g2 * C + c] : 0.0;
+      for (int g = 0; g < G; ++g)
+        acc += __ldg(slgg + (((size_t)g * nmat + mt) * G + g2) * nmom + l) *
+               sq[(g * CELLS + cc) * M + m];
+      PT *dst = phib + ((size_t)g2 * C + c) * M + m;
+      const PT nv = (PT)acc;
+      const double d = fabs((double)nv - (double)*dst);
+      md = (d != d) ? INFINITY : fmax(md, d);
+      ma = fmax(ma, fabs((double)nv));
+      *dst = nv;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    md = fmax(md, __shfl_xor_sync(0xffffffffu, md, o));
+    ma = fmax(ma, __shfl_xor_sync(0xffffffffu, ma, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(norm, (unsigned long long)__double_as_longlong(md));
+    atomicMax(norm + 1, (unsigned long long)__double_as_longlong(ma));
+  }
+}
+
+template <typename QT>
+__global__ void grad_sxs_kernel(const QT *__restrict__ qbar, const double *__restrict__ flux,
                                 double *__restrict__ grad, int G, int nmom, int M, long long C) {
   const long long n = (long long)G * C * nmom;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
@@ -255,12 +305,14 @@ __global__ void grad_sxs_kernel(const double *__restrict__ qbar, const double *_
     const int l = (int)(i % nmom);
     const long long gc = i / nmom;
     double acc = 0.0;
-    for (int k = l * l; k < (l + 1) * (l + 1) && k < M; ++k) acc += qbar[gc * M + k] * flux[gc * M + k];
+    for (int k = l * l; k < (l + 1) * (l + 1) && k < M; ++k)
+      acc += (double)qbar[gc * M + k] * flux[gc * M + k];
     grad[i] = acc;
   }
 }
 
-__global__ void moment0_kernel(const double *__restrict__ in, double *__restrict__ out, int M,
+template <typename IT>
+__global__ void moment0_kernel(const IT *__restrict__ in, double *__restrict__ out, int M,
                                long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
@@ -320,12 +372,54 @@ cudaError_t k_adjoint_scatter(const double *r, const double *slgg, const int32_t
 
 cudaError_t k_grad_sxs(const double *qbar, const double *flux, double *grad, int G, int nmom,
                        int M, long long C, cudaStream_t st) {
-  grad_sxs_kernel<<<grid_for((long long)G * C * nmom), BLK, 0, st>>>(qbar, flux, grad, G, nmom, M, C);
+  return k_grad_sxs_any(qbar, 0, flux, grad, G, nmom, M, C, st);
+}
+
+cudaError_t k_grad_sxs_any(const void *qbar, int fp32, const double *flux, double *grad, int G,
+                           int nmom, int M, long long C, cudaStream_t st) {
+  const int grid = grid_for((long long)G * C * nmom);
+  if (fp32)
+    grad_sxs_kernel<float><<<grid, BLK, 0, st>>>((const float *)qbar, flux, grad, G, nmom, M, C);
+  else
+    grad_sxs_kernel<double><<<grid, BLK, 0, st>>>((const double *)qbar, flux, grad, G, nmom, M, C);
   return cudaGetLastError();
 }
 
 cudaError_t k_moment0(const double *in, double *out, int M, long long n, cudaStream_t st) {
-  moment0_kernel<<<grid_for(n), BLK, 0, st>>>(in, out, M, n);
+  moment0_kernel<double><<<grid_for(n), BLK, 0, st>>>(in, out, M, n);
+  return cudaGetLastError();
+}
+
+cudaError_t k_moment0_any(const void *in, int fp32, double *out, int M, long long n,
+                          cudaStream_t st) {
+  if (fp32)
+    moment0_kernel<float><<<grid_for(n), BLK, 0, st>>>((const float *)in, out, M, n);
+  else
+    moment0_kernel<double><<<grid_for(n), BLK, 0, st>>>((const double *)in, out, M, n);
+  return cudaGetLastError();
+}
+
+cudaError_t k_adjoint_update(const double *r, const double *slgg, const int32_t *mat,
+                             const void *qbar, void *phib, int fp32, unsigned long long *norm,
+                             int G, int nmat, int nmom, int M, long long C, cudaStream_t st) {
+  constexpr int CELLS = 4;
+  const size_t smem = sizeof(double) * G * CELLS * M;
+  if (smem > 200 * 1024) return cudaErrorInvalidValue;
+  const long long tiles = (C + CELLS - 1) / CELLS;
+  cudaError_t e;
+  if (fp32) {
+    auto kern = adjoint_update_kernel<CELLS, float, float>;
+    if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
+      return e;
+    kern<<<grid_for(tiles, 1), BLK, smem, st>>>(r, slgg, mat, (const float *)qbar, (float *)phib,
+                                                norm, G, nmat, nmom, M, C);
+  } else {
+    auto kern = adjoint_update_kernel<CELLS, double, double>;
+    if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
+      return e;
+    kern<<<grid_for(tiles, 1), BLK, smem, st>>>(r, slgg, mat, (const double *)qbar,
+                                                (double *)phib, norm, G, nmat, nmom, M, C);
+  }
   return cudaGetLastError();
 }
 

@@ -36,13 +36,22 @@ std::vector<double> trigint(bool cos_form, int n, double d, double del, const st
   return fn;
 }
 
-// Cell edges starting at 0 with step `step` (mms.cc:104-112; the reference
-// steps y and z by dx too, which the caller reproduces).
-std::vector<double> edges(int n, double step) {
-  std::vector<double> b(n + 1);
-  b[0] = 0.0;
-  for (int i = 1; i <= n; ++i) b[i] = b[i - 1] + step;
-  return b;
+// The cell integrals along one axis of n cells split into chunks of `per`
+// cells, as each chunk's task computes them (mms.cc:101-121, 240-275): the
+// chunk's first edge is its first global cell index times the axis's own
+// spacing `del`, the next ones step by `step` (the reference steps every axis
+// by dx, which the caller passes), and the integrals use `del`.
+std::vector<double> axis_trig(bool cos_form, int n, int per, double d, double del, double step) {
+  std::vector<double> fn;
+  fn.reserve(n);
+  std::vector<double> b(per + 1);
+  for (int lo = 0; lo < n; lo += per) {
+    b[0] = lo * del;
+    for (int i = 1; i <= per; ++i) b[i] = b[i - 1] + step;
+    const std::vector<double> f = trigint(cos_form, per, d, del, b);
+    fn.insert(fn.end(), f.begin(), f.end());
+  }
+  return fn;
 }
 
 // ref[g][c] = (g+1) tx[i] ty[j] tz[k]  (mms.cc:131-149)
@@ -165,11 +174,11 @@ cudaError_t mms_init(const MmsGeometry &geo, const int32_t *mat, const double *s
   const double a = kPi / geo.lx, b = kPi / geo.ly, c = kPi / geo.lz;
   const double dx = geo.lx / double(nx), dy = geo.ly / double(ny), dz = geo.lz / double(nz);
   // the reference steps all three axes' edges by dx (mms.cc:104-112, 240-249)
-  const std::vector<double> ib = edges(nx, dx), jb = edges(ny, dx), kb = edges(nz, dx);
   std::vector<double> host;
-  const auto cx = trigint(true, nx, a, dx, ib), sx = trigint(false, nx, a, dx, ib);
-  const auto cy = trigint(true, ny, b, dy, jb), sy = trigint(false, ny, b, dy, jb);
-  const auto cz = trigint(true, nz, c, dz, kb), sz = trigint(false, nz, c, dz, kb);
+  const int *pc = geo.chunk;
+  const auto cx = axis_trig(true, nx, pc[0], a, dx, dx), sx = axis_trig(false, nx, pc[0], a, dx, dx);
+  const auto cy = axis_trig(true, ny, pc[1], b, dy, dx), sy = axis_trig(false, ny, pc[1], b, dy, dx);
+  const auto cz = axis_trig(true, nz, pc[2], c, dz, dx), sz = axis_trig(false, nz, pc[2], c, dz, dx);
   for (const auto *v : {&cx, &sx, &cy, &sy, &cz, &sz}) host.insert(host.end(), v->begin(), v->end());
   for (int q = 0; q < 3; ++q) host.insert(host.end(), geo.quad[q], geo.quad[q] + geo.A);
   // scratch: [trig 2nx+2ny+2nz][mu eta xi 3A]

@@ -71,7 +71,9 @@ struct snap_ctx {
   double *d_old0 = nullptr;        // [G][C] scalar flux before the current inner sweep
   bool atomic_octants = true;      // inner iterations add octants straight into the flux
   void *d_slots = nullptr, *d_bx = nullptr, *d_by = nullptr;
-  size_t slots_bytes = 0;   // octant slots: allocated on first use (inner iterations need none)
+  size_t slots_bytes = 0;   // octant slots of every group (inner iterations need none)
+  size_t slots_alloc = 0;   // bytes of octant slots allocated (first use, sized to its groups)
+  size_t sbar_alloc = 0;    // bytes of sigma_t adjoint slots allocated
   int *d_ctrl = nullptr;   // [n_items * TY progress][counter][error][violations]
   int *h_ctrl = nullptr;   // pinned: error, violations, largest change (float bits)
   float prev_inner_df = 0.0f;   // FP32 contexts: largest change of the previous inner iteration
@@ -90,6 +92,7 @@ struct snap_ctx {
   int state_groups = 0;
   struct BatchTables {
     int n_items = 0;
+    int P = 1;   // octants per launch of a batch (more than the context's when the faces allow)
     int *table = nullptr, *index = nullptr;
   };
   std::vector<BatchTables> batch_tables;
@@ -321,13 +324,22 @@ int sweep_launches(snap_ctx *c, const void *qtot, const void *t_xs, cudaStream_t
   p.item_index = batch ? c->batch_tables[gn].index : c->d_item_index;
   p.qtot = (const char *)qtot + (size_t)g0 * c->C * c->M * c->wsize;
   p.t_xs = (const char *)t_xs + (size_t)g0 * c->C * c->wsize;
-  if (!atomic_flux && !c->d_slots) {
-    if (cudaMalloc(&c->d_slots, c->slots_bytes) != cudaSuccess) {
-      cudaGetLastError();
-      c->d_slots = nullptr;
-      return fail(SNAP_ERR_OOM, "cannot allocate the octant flux slots");
+  const int P = batch ? c->batch_tables[gn].P : c->P;   // octants per launch
+  if (!atomic_flux) {
+    // octant slots for the groups of this launch (first use allocates)
+    const size_t need = (size_t)P * p.G * c->C * c->M * c->wsize;
+    if (!c->d_slots || c->slots_alloc < need) {
+      cudaFree(c->d_slots);
+      c->scratch_bytes -= c->slots_alloc;
+      c->slots_alloc = 0;
+      if (cudaMalloc(&c->d_slots, need) != cudaSuccess) {
+        cudaGetLastError();
+        c->d_slots = nullptr;
+        return fail(SNAP_ERR_OOM, "cannot allocate the octant flux slots");
+      }
+      c->slots_alloc = need;
+      c->scratch_bytes += need;
     }
-    c->scratch_bytes += c->slots_bytes;
   }
   p.phi_slots = atomic_flux ? (void *)atomic_flux : c->d_slots;
   p.atomic_flux = atomic_flux ? 1 : 0;
@@ -362,8 +374,8 @@ int sweep_launches(snap_ctx *c, const void *qtot, const void *t_xs, cudaStream_t
     grid = std::min(blocks * sms, p.n_items);
   }
   if (batch) grid = std::min(grid, p.n_items);
-  for (int L = 0; L < 8 / c->P; ++L) {
-    p.o_base = L * c->P;
+  for (int L = 0; L < 8 / P; ++L) {
+    p.o_base = L * P;
     p.accumulate = L > 0;
     SNAP_CUDA(cudaMemsetAsync(c->d_ctrl, 0, sizeof(int) * (c->n_progress() + 1), st));
     cudaError_t e;
@@ -1135,8 +1147,9 @@ done:
 extern "C" {
 
 int snap_mms_init(snap_ctx *c, const int32_t *mat, const double *sigt, const double *slgg,
-                  double lx, double ly, double lz, int timedep, double tf, double dt,
-                  double *ref_flux, double *qim, double *qi, void *stream) {
+                  double lx, double ly, double lz, const int *chunk_cells, int timedep,
+                  double tf, double dt, double *ref_flux, double *qim, double *qi,
+                  void *stream) {
   if (!c || !mat || !sigt || !slgg || !ref_flux || !qim || (timedep && !qi))
     return fail(SNAP_ERR_BAD_ARG, "null argument");
   if (c->cfg.nmom != 1)
@@ -1160,6 +1173,12 @@ int snap_mms_init(snap_ctx *c, const int32_t *mat, const double *sigt, const dou
   geo.quad[0] = c->mu.data();
   geo.quad[1] = c->eta.data();
   geo.quad[2] = c->xi.data();
+  const int dims[3] = {geo.nx, geo.ny, geo.nz};
+  for (int d = 0; d < 3; ++d) {
+    geo.chunk[d] = chunk_cells ? chunk_cells[d] : dims[d];
+    if (geo.chunk[d] < 1 || dims[d] % geo.chunk[d])
+      return fail(SNAP_ERR_BAD_ARG, "chunk_cells must divide the mesh");
+  }
   double *scratch = nullptr;
   const size_t words = mms_scratch_words(geo.nx, geo.ny, geo.nz, geo.A);
   SNAP_CUDA(cudaMalloc((void **)&scratch, sizeof(double) * words));
@@ -1238,8 +1257,13 @@ int ensure_batch_tables(snap_ctx *c, int gn) {
   if ((int)c->batch_tables.size() <= gn) c->batch_tables.resize(gn + 1);
   auto &b = c->batch_tables[gn];
   if (b.table) return SNAP_OK;
+  // as many octants per launch as the tile-face scratch (sized for the
+  // context's P octants of every group) holds for gn groups
+  int P = 8;
+  while (P > c->P && (size_t)P * gn > (size_t)c->P * c->cfg.ng) P /= 2;
+  b.P = P;
   std::vector<int> table, index;
-  build_items(c->P, gn, c->tiles_x, c->tiles_y, table, index);
+  build_items(P, gn, c->tiles_x, c->tiles_y, table, index);
   int rc;
   if ((rc = upload((void **)&b.table, table)) || (rc = upload((void **)&b.index, index))) return rc;
   b.n_items = (int)table.size();
@@ -1271,34 +1295,44 @@ int ensure_state(snap_ctx *c, int groups = 0) {
   return SNAP_OK;
 }
 
-int ensure_sbar(snap_ctx *c) {
-  if (c->d_sbar_slots) return SNAP_OK;
-  const size_t n = (size_t)c->P * c->cfg.ng * c->C;
-  if (cudaMalloc(&c->d_sbar_slots, n * c->wsize) != cudaSuccess) {
+int ensure_sbar(snap_ctx *c, int groups, int P) {
+  const size_t need = (size_t)P * groups * c->C * c->wsize;
+  if (c->d_sbar_slots && c->sbar_alloc >= need) return SNAP_OK;
+  cudaFree(c->d_sbar_slots);
+  c->scratch_bytes -= c->sbar_alloc;
+  c->sbar_alloc = 0;
+  if (cudaMalloc(&c->d_sbar_slots, need) != cudaSuccess) {
     cudaGetLastError();
+    c->d_sbar_slots = nullptr;
     return fail(SNAP_ERR_OOM, "cannot allocate the sigma_t adjoint slots");
   }
-  c->scratch_bytes += n * c->wsize;
+  c->sbar_alloc = need;
+  c->scratch_bytes += need;
   return SNAP_OK;
 }
 
-int adjoint_sweep_impl(snap_ctx *c, const void *phi_bar, const void *t_xs, double *qtot_bar,
-                       double *sigt_bar, cudaStream_t st, int g0 = 0, int gn = 0) {
+// qtot_bar: double [G][C][M], or float when qbar_fp32 (FP32 contexts' lean
+// adjoint solve)
+int adjoint_sweep_impl(snap_ctx *c, const void *phi_bar, const void *t_xs, void *qtot_bar,
+                       double *sigt_bar, cudaStream_t st, int g0 = 0, int gn = 0,
+                       int qbar_fp32 = 0) {
   const int groups = gn > 0 ? gn : c->cfg.ng;
   if ((sigt_bar || c->cfg.fixup) && (!c->state_recorded || c->state_groups < groups))
     return fail(SNAP_ERR_BAD_ARG, "record the forward state (snap_record_forward) first");
+  const int P = (gn > 0 && gn < c->cfg.ng) ? c->batch_tables[gn].P : c->P;
   int rc;
-  if (sigt_bar && (rc = ensure_sbar(c))) return rc;
+  if (sigt_bar && (rc = ensure_sbar(c, groups, P))) return rc;
   SNAP_CUDA(cudaEventRecord(c->sw0, st));
   rc = sweep_launches(c, phi_bar, t_xs, st, 2, sigt_bar ? c->d_sbar_slots : nullptr, nullptr, g0,
                       gn);
   if (rc) return rc;
   SNAP_CUDA(cudaEventRecord(c->sw1, st));
-  SNAP_CUDA(k_reduce_slots(c->d_slots, c->P, c->fp32, qtot_bar + (size_t)g0 * c->C * c->M, 0,
-                           nullptr, groups, c->M, c->C, 0, 0.0, nullptr, st));
+  void *qb = (char *)qtot_bar + (size_t)g0 * c->C * c->M * (qbar_fp32 ? sizeof(float) : sizeof(double));
+  SNAP_CUDA(k_reduce_slots(c->d_slots, P, c->fp32, qb, qbar_fp32, nullptr, groups, c->M, c->C,
+                           0, 0.0, nullptr, st));
   ++c->launches;
   if (sigt_bar) {
-    SNAP_CUDA(k_reduce_slots(c->d_sbar_slots, c->P, c->fp32, sigt_bar + (size_t)g0 * c->C, 0,
+    SNAP_CUDA(k_reduce_slots(c->d_sbar_slots, P, c->fp32, sigt_bar + (size_t)g0 * c->C, 0,
                              nullptr, groups, 1, c->C, 0, 0.0, nullptr, st));
     ++c->launches;
   }
@@ -1309,14 +1343,15 @@ int adjoint_sweep_impl(snap_ctx *c, const void *phi_bar, const void *t_xs, doubl
 // with the forward state recorded from `qtot` batch by batch when the
 // context holds the state of fewer groups than it sweeps.
 int adjoint_apply(snap_ctx *c, const void *phi_bar, const void *t_xs, const void *qtot,
-                  double *qtot_bar, double *sigt_bar, cudaStream_t st, int batch) {
+                  void *qtot_bar, double *sigt_bar, cudaStream_t st, int batch, int qbar_fp32) {
   const int G = c->cfg.ng;
-  if (batch >= G) return adjoint_sweep_impl(c, phi_bar, t_xs, qtot_bar, sigt_bar, st);
+  if (batch >= G)
+    return adjoint_sweep_impl(c, phi_bar, t_xs, qtot_bar, sigt_bar, st, 0, 0, qbar_fp32);
   for (int g0 = 0; g0 < G; g0 += batch) {
     const int gn = std::min(batch, G - g0);
     int rc = sweep_launches(c, qtot, t_xs, st, 1, nullptr, nullptr, g0, gn);
     if (rc) return rc;
-    rc = adjoint_sweep_impl(c, phi_bar, t_xs, qtot_bar, sigt_bar, st, g0, gn);
+    rc = adjoint_sweep_impl(c, phi_bar, t_xs, qtot_bar, sigt_bar, st, g0, gn, qbar_fp32);
     if (rc) return rc;
   }
   return SNAP_OK;
@@ -1369,29 +1404,30 @@ int snap_adjoint_solve(snap_ctx *c, const int32_t *mat, const double *qi, const 
   cudaStream_t st = (cudaStream_t)stream;
   const int G = c->cfg.ng, M = c->M, nmom = c->cfg.nmom;
   const long long C = c->C, n = (long long)G * C;
-  double *t_xs64 = nullptr, *s_xs = nullptr, *q2grp = nullptr, *qbar = nullptr, *pb = nullptr,
-         *pb2 = nullptr;
-  void *qtot = nullptr, *t_xs_sw = nullptr, *pb_sw = nullptr;
+  const int f32 = c->fp32;
+  // Work arrays: the context's solve arrays (total source, in-group
+  // scattering, sweep-precision t_xs), and the adjoint vectors phi_bar and
+  // qtot_bar in the sweep precision.  In FP32 contexts both fit in the space
+  // of the FP64 outer-source array, which is free once the total source is
+  // formed; FP64 contexts add one array for qtot_bar.
+  int rc = ensure_solve_arrays(c);
+  if (rc) return rc;
+  double *qbar64 = nullptr;
   unsigned long long *d_norm = nullptr;
-  auto cleanup = [&]() {
-    cudaFree(t_xs64); cudaFree(s_xs); cudaFree(q2grp); cudaFree(qbar); cudaFree(pb);
-    cudaFree(pb2); cudaFree(qtot); cudaFree(d_norm);
-    if (c->fp32) { cudaFree(t_xs_sw); cudaFree(pb_sw); }
-  };
-  if (cudaMalloc(&t_xs64, sizeof(double) * n) != cudaSuccess ||
-      cudaMalloc(&s_xs, sizeof(double) * n * nmom) != cudaSuccess ||
-      cudaMalloc(&q2grp, sizeof(double) * n * M) != cudaSuccess ||
-      cudaMalloc(&qbar, sizeof(double) * n * M) != cudaSuccess ||
-      cudaMalloc(&pb, sizeof(double) * n * M) != cudaSuccess ||
-      cudaMalloc(&pb2, sizeof(double) * n * M) != cudaSuccess ||
-      cudaMalloc(&qtot, c->wsize * n * M) != cudaSuccess ||
-      cudaMalloc((void **)&d_norm, 2 * sizeof(unsigned long long)) != cudaSuccess ||
-      (c->fp32 && cudaMalloc(&t_xs_sw, sizeof(float) * n) != cudaSuccess) ||
-      (c->fp32 && cudaMalloc(&pb_sw, sizeof(float) * n * M) != cudaSuccess)) {
+  if ((!f32 && cudaMalloc((void **)&qbar64, sizeof(double) * n * M) != cudaSuccess) ||
+      cudaMalloc((void **)&d_norm, 2 * sizeof(unsigned long long)) != cudaSuccess) {
     cudaGetLastError();
-    cleanup();
+    cudaFree(qbar64);
     return fail(SNAP_ERR_OOM, "cannot allocate adjoint solve arrays");
   }
+  auto cleanup = [&]() {
+    cudaFree(qbar64);
+    cudaFree(d_norm);
+  };
+  void *pb = c->s_q2;                                        // phi_bar [G][C][M]
+  void *qbar = f32 ? (void *)((float *)c->s_q2 + n * M) : (void *)qbar64;
+  const void *t_sw = f32 ? c->s_txsw : (const void *)t_xs;
+  void *qtot = c->s_qtot;
   // forward state of `batch` groups at a time: all groups when it fits in
   // 70 % of the free memory (recorded once), else batches recorded again
   // from the converged flux moments for every adjoint iteration
@@ -1399,13 +1435,14 @@ int snap_adjoint_solve(snap_ctx *c, const int32_t *mat, const double *qi, const 
   {
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
-    const size_t per_group = (size_t)8 * C * c->AP * (c->wsize + 1);
+    const size_t per_group = (size_t)8 * C * c->AP * (c->wsize + 1) +     // recorded state
+                             (size_t)c->P * C * (M + 1) * c->wsize;         // octant slots
     const size_t held = c->d_pc_store ? (size_t)c->state_groups * per_group : 0;
     const size_t avail = (size_t)(0.7 * (double)(free_b + held));
     batch = (int)std::max<size_t>(1, std::min<size_t>((size_t)G, avail / per_group));
     if (const char *e = getenv("SNAP_B200_ADJOINT_GROUPS")) batch = std::max(1, std::min(G, atoi(e)));
   }
-  int rc = ensure_state(c, batch);
+  rc = ensure_state(c, batch);
   if (!rc && batch < G) {
     rc = ensure_batch_tables(c, batch);
     if (!rc && G % batch) rc = ensure_batch_tables(c, G % batch);
@@ -1430,44 +1467,40 @@ int snap_adjoint_solve(snap_ctx *c, const int32_t *mat, const double *qi, const 
     ASTEP(cudaMemsetAsync(c->error(), 0, 2 * sizeof(int), st));
     ASTEP(cudaEventRecord(c->ev0, st));
     // the forward operator at the converged flux: total source
-    ASTEP(cudaMemcpyAsync(t_xs64, t_xs, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-    ASTEP(k_expand_scat(slgg, mat, s_xs, G, c->cfg.nmat, nmom, C, st));
-    if (c->fp32) ASTEP(k_to_f32(t_xs64, (float *)t_xs_sw, n, st));
-    ASTEP(k_outer_source(qi, slgg, mat, flux, q2grp, G, c->cfg.nmat, nmom, M, C, st));
-    ASTEP(k_inner_source(s_xs, q2grp, flux, qtot, c->fp32, G, nmom, M, C, st));
-    c->launches += c->fp32 ? 4 : 3;
+    ASTEP(k_expand_scat(slgg, mat, c->s_sxs, G, c->cfg.nmat, nmom, C, st));
+    if (f32) ASTEP(k_to_f32(t_xs, (float *)c->s_txsw, n, st));
+    ASTEP(k_outer_source(qi, slgg, mat, flux, c->s_q2, G, c->cfg.nmat, nmom, M, C, st));
+    ASTEP(k_inner_source(c->s_sxs, c->s_q2, flux, qtot, f32, G, nmom, M, C, st));
+    c->launches += f32 ? 4 : 3;
     // forward sweep recording the cell-average fluxes and fixup flags (with
     // batches: recorded inside every adjoint application)
     if (batch >= G) {
-      rc = sweep_launches(c, qtot, c->fp32 ? t_xs_sw : t_xs64, st, 1);
+      rc = sweep_launches(c, qtot, t_sw, st, 1);
       if (rc) goto adone;
     }
     c->state_recorded = true;
     // adjoint source iteration: phi_bar = r + S^T M^T L^-T D^T phi_bar,
     // converged when max|change| <= epsi * max|phi_bar| (the adjoint spans
-    // many decades, so the forward test's per-cell form does not apply)
-    ASTEP(cudaMemsetAsync(qbar, 0, sizeof(double) * n * M, st));
-    ASTEP(k_adjoint_scatter(response, slgg, mat, qbar, pb, G, c->cfg.nmat, nmom, M, C, st));
+    // many decades, so the forward test's per-cell form does not apply);
+    // phi_bar starts at r (qtot_bar = 0)
+    ASTEP(cudaMemsetAsync(qbar, 0, (f32 ? sizeof(float) : sizeof(double)) * n * M, st));
+    ASTEP(cudaMemsetAsync(pb, 0, (f32 ? sizeof(float) : sizeof(double)) * n * M, st));
+    ASTEP(cudaMemsetAsync(d_norm, 0, 2 * sizeof(unsigned long long), st));
+    ASTEP(k_adjoint_update(response, slgg, mat, qbar, pb, f32, d_norm, G, c->cfg.nmat, nmom, M, C,
+                           st));
     ++c->launches;
     for (int it = 0; it < maxit; ++it) {
-      const void *src = pb;
-      if (c->fp32) {
-        ASTEP(k_to_f32(pb, (float *)pb_sw, n * M, st));
-        ++c->launches;
-        src = pb_sw;
-      }
-      rc = adjoint_apply(c, src, c->fp32 ? t_xs_sw : t_xs64, qtot, qbar, nullptr, st, batch);
+      rc = adjoint_apply(c, pb, t_sw, qtot, qbar, nullptr, st, batch, f32);
       if (rc) goto adone;
-      ASTEP(k_adjoint_scatter(response, slgg, mat, qbar, pb2, G, c->cfg.nmat, nmom, M, C, st));
       ASTEP(cudaMemsetAsync(d_norm, 0, 2 * sizeof(unsigned long long), st));
-      ASTEP(k_max_abs_diff(pb2, pb, n * M, d_norm, st));
-      c->launches += 2;
+      ASTEP(k_adjoint_update(response, slgg, mat, qbar, pb, f32, d_norm, G, c->cfg.nmat, nmom, M,
+                             C, st));
+      ++c->launches;
       unsigned long long hn[2] = {0, 0};
       ASTEP(cudaMemcpyAsync(hn, d_norm, sizeof(hn), cudaMemcpyDeviceToHost, st));
       rc = read_ctrl(c, st, nullptr);
       if (rc) goto adone;
       account_sweep(c);
-      std::swap(pb, pb2);
       ++info->inner_total;
       double dmax, amax;
       memcpy(&dmax, &hn[0], sizeof(double));
@@ -1479,18 +1512,10 @@ int snap_adjoint_solve(snap_ctx *c, const int32_t *mat, const double *qi, const 
     }
     info->outer_total = 1;
     // gradients from the converged adjoint
-    {
-      const void *src = pb;
-      if (c->fp32) {
-        ASTEP(k_to_f32(pb, (float *)pb_sw, n * M, st));
-        ++c->launches;
-        src = pb_sw;
-      }
-      rc = adjoint_apply(c, src, c->fp32 ? t_xs_sw : t_xs64, qtot, qbar, grad_sigt, st, batch);
-      if (rc) goto adone;
-    }
-    ASTEP(k_moment0(qbar, grad_qi, M, n, st));
-    if (grad_sxs) ASTEP(k_grad_sxs(qbar, flux, grad_sxs, G, nmom, M, C, st));
+    rc = adjoint_apply(c, pb, t_sw, qtot, qbar, grad_sigt, st, batch, f32);
+    if (rc) goto adone;
+    ASTEP(k_moment0_any(qbar, f32, grad_qi, M, n, st));
+    if (grad_sxs) ASTEP(k_grad_sxs_any(qbar, f32, flux, grad_sxs, G, nmom, M, C, st));
     c->launches += grad_sxs ? 2 : 1;
     rc = read_ctrl(c, st, nullptr);
     if (rc) goto adone;

@@ -83,7 +83,7 @@ SIGNATURES = {
     "snap_sweep_noalloc": [C.POINTER(SnapConfig), _vp, _vp, _vp, _vp],
     "snap_inject_stall": [_vp, C.c_int],
     "snap_sweep_td": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
-    "snap_mms_init": [_vp, _vp, _vp, _vp, C.c_double, C.c_double, C.c_double, C.c_int,
+    "snap_mms_init": [_vp, _vp, _vp, _vp, C.c_double, C.c_double, C.c_double, _vp, C.c_int,
                       C.c_double, C.c_double, _vp, _vp, _vp, _vp],
     "snap_mms_compare": [_vp, _vp, _vp, _vp, _vp],
     "snap_selftest_division": [C.c_int, _vp, _vp, C.c_longlong, _vp, _vp],

@@ -17,6 +17,16 @@ MAX_LIMIT = 0.1     # snap.cc:551-554
 AVG_LIMIT = 1e-3    # snap.cc:555-558
 
 
+def avg_divisor(d: Deck) -> int:
+    """The divisor of the reference's average difference: the global cell
+    count times the number of spatial chunks times the groups (snap.cc:547-548
+    multiplies the global nx, ny, nz by the chunk counts), so a 2x2x2-chunk
+    deck reports an average 8 times smaller than the same deck in one
+    chunk."""
+    npey, npez, ichunk = d.chunks
+    return d.cells * ichunk * npey * npez * d.ng
+
+
 def mms_solve(d: Deck, device: int = 0):
     """Solves the deck's manufactured problem; returns the flux moments, the
     iteration record and {max, min, sum, avg} of |flux/ref - 1|."""
@@ -30,16 +40,18 @@ def mms_solve(d: Deck, device: int = 0):
         ref = torch.empty(d.ng, d.cells, dtype=torch.float64, device=dev)
         qim = torch.empty(8, d.ng, d.cells, d.nang, dtype=torch.float64, device=dev)
         qi = torch.zeros(d.ng, d.cells, dtype=torch.float64, device=dev)
+        npey, npez, ichunk = d.chunks
+        chunk_cells = (C.c_int * 3)(d.nx // ichunk, d.ny // npey, d.nz // npez)
         abi.check(snap.lib.snap_mms_init(
             snap.handle, _ptr(dp["mat"]), _ptr(dp["sigt"]), _ptr(dp["slgg"]), C.c_double(d.lx),
-            C.c_double(d.ly), C.c_double(d.lz), int(d.timedep), C.c_double(d.tf),
+            C.c_double(d.ly), C.c_double(d.lz), chunk_cells, int(d.timedep), C.c_double(d.tf),
             C.c_double(d.dt), _ptr(ref), _ptr(qim), _ptr(qi), _stream()))
         dp["qi"] = qi                  # steady state: no fixed source (snap.cc:351-355)
         dp["qim"] = qim
         flux, rec = snap.transport_solve(dp)
         out = (C.c_double * 3)()
         abi.check(snap.lib.snap_mms_compare(snap.handle, _ptr(flux), _ptr(ref), out, _stream()))
-        res = dict(max=out[0], min=out[1], sum=out[2], avg=out[2] / (d.cells * d.ng))
+        res = dict(max=out[0], min=out[1], sum=out[2], avg=out[2] / avg_divisor(d))
         return flux, rec, res, ref
     finally:
         snap.close()

@@ -47,8 +47,10 @@ class Deck:
     # None: the benchmark rule of make_problem
     mat_opt: int | None = None
     src_opt: int | None = None
-    # spatial chunks of the reference deck (npey, npez, ichunk); this build
-    # sweeps the whole mesh in one domain, so they only describe the deck
+    # spatial chunks of the reference deck (npey, npez, ichunk); the sweep
+    # covers the whole mesh as one domain (chunked and one-chunk reference
+    # runs agree to rounding); they set the MMS check's per-chunk cell edges
+    # and the divisor of its average
     chunks: tuple = (1, 1, 1)
 
     @property

@@ -170,13 +170,14 @@ class Snap:
         return qbar, sbar
 
     def adjoint_solve(self, dprob: dict, t_xs: torch.Tensor, flux: torch.Tensor,
-                      response: torch.Tensor, epsi=None, maxit=None) -> dict:
-        """dJ/dt_xs, dJ/dqi and dJ/ds_xs of J = sum response * scalar flux at
-        the converged forward flux (discrete adjoint, fixup flags frozen)."""
+                      response: torch.Tensor, epsi=None, maxit=None, with_sxs: bool = True) -> dict:
+        """dJ/dt_xs, dJ/dqi and (with_sxs) dJ/ds_xs of J = sum response *
+        scalar flux at the converged forward flux (discrete adjoint, fixup
+        flags frozen)."""
         d = self.deck
         gs = self._empty(d.ng, self.C)
         gq = self._empty(d.ng, self.C)
-        gx = self._empty(d.ng, self.C, d.nmom)
+        gx = self._empty(d.ng, self.C, d.nmom) if with_sxs else None
         info = abi.SnapSolveInfo()
         info.epsi = d.epsi if epsi is None else epsi
         info.iitm = 1
@@ -184,7 +185,7 @@ class Snap:
         abi.check(self.lib.snap_adjoint_solve(
             self.handle, _ptr(dprob["mat"]), _ptr(dprob["qi"]), _ptr(t_xs.contiguous()),
             _ptr(dprob["slgg"]), _ptr(flux), _ptr(response.contiguous()), _ptr(gs), _ptr(gq),
-            _ptr(gx), C.byref(info), _stream()))
+            _ptr(gx) if gx is not None else None, C.byref(info), _stream()))
         return dict(grad_sigt=gs, grad_qi=gq, grad_sxs=gx, iterations=info.inner_total,
                     converged=bool(info.converged), total_ms=info.total_ms,
                     sweep_ms=info.sweep_ms)

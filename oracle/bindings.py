@@ -157,11 +157,14 @@ class RefSnap:
             # a reference deck: its layouts, lengths and time stepping
             mat_opt = 1 if deck.mat_opt is None else deck.mat_opt
             src_opt = 1 if deck.src_opt is None else deck.src_opt
+            # the deck's spatial chunks (npey, npez, ichunk): the reference's
+            # sweep runs one task per chunk, faces passed between them
+            npey, npez, ichunk = deck.chunks
             rc = self.lib.snapref_configure_deck(
                 deck.nx, deck.ny, deck.nz, C.c_double(deck.lx), C.c_double(deck.ly),
                 C.c_double(deck.lz), deck.nang, deck.ng, deck.nmom, C.c_double(deck.epsi),
                 deck.iitm, deck.oitm, int(deck.fixup), int(deck.timedep), C.c_double(deck.tf),
-                deck.nsteps, mat_opt, src_opt)
+                deck.nsteps, mat_opt, src_opt, ichunk, npey, npez)
         if rc != 0:
             raise RuntimeError(f"reference configuration failed: {rc}")
 
@@ -231,6 +234,6 @@ class RefSnap:
                    nthreads=nthreads)
         if d.src_opt == 3:
             rec["mms"] = dict(max=float(mms[0]), min=float(mms[1]), sum=float(mms[2]),
-                              avg=float(mms[2]) / (d.cells * d.ng))
+                              avg=float(mms[2]) / (d.cells * int(np.prod(d.chunks)) * d.ng))
             rec["ref_flux"] = ref_flux
         return flux, rec

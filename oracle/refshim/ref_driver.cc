@@ -179,10 +179,15 @@ PhysicalRegion map_store(const Store &s) {
 
 Runtime g_runtime;
 
-/* Executes one point of an index launch built by a reference task ctor. */
+/* Executes one point of an index launch built by a reference task ctor.
+ * chunk: the point's spatial chunk (the sub-box its 3-D region requirements
+ * project to, snap.cc:56-62); NULL for the whole space.  2-D (face) and 1-D
+ * requirements see their whole space, which the task indexes with global
+ * points (sweep.cc:217-239). */
 template <typename RET>
 RET execute(const IndexTaskLauncher &launcher,
-            RET (*impl)(const Task *, const std::vector<PhysicalRegion> &, Context, Runtime *)) {
+            RET (*impl)(const Task *, const std::vector<PhysicalRegion> &, Context, Runtime *),
+            const Legion::IndexSpace *chunk = nullptr) {
   Task task;
   task.args = launcher.global_arg.args;
   task.arglen = launcher.global_arg.arglen;
@@ -191,7 +196,7 @@ RET execute(const IndexTaskLauncher &launcher,
   for (const RegionRequirement &rr : launcher.region_requirements) {
     RegionRequirement r = rr;
     const Store &s = g_stores[rr.region.handle];
-    r.region.is = s.is; /* single spatial chunk: the point's subregion is the whole space */
+    r.region.is = (chunk && s.is.dim == 3) ? *chunk : s.is;
     task.regions.push_back(r);
     regions.push_back(map_store(s));
   }
@@ -315,6 +320,29 @@ template <typename F> void parallel_for(int n, int nthreads, F f) {
   for (auto &t : th) t.join();
 }
 
+/* The spatial chunk boxes (snap.cc:56-62 blockify): calls f(box) for every
+ * chunk, x fastest, or f(nullptr) once when the mesh is one chunk. */
+template <typename F> void for_each_chunk(F f) {
+  const int nc[3] = {Snap::nx_chunks, Snap::ny_chunks, Snap::nz_chunks};
+  if (nc[0] * nc[1] * nc[2] == 1) {
+    f((const Legion::IndexSpace *)nullptr);
+    return;
+  }
+  const int per[3] = {Snap::nx_per_chunk, Snap::ny_per_chunk, Snap::nz_per_chunk};
+  for (int kz = 0; kz < nc[2]; kz++)
+    for (int ky = 0; ky < nc[1]; ky++)
+      for (int kx = 0; kx < nc[0]; kx++) {
+        const int ck[3] = {kx, ky, kz};
+        Legion::IndexSpace box;
+        box.dim = 3;
+        for (int d = 0; d < 3; d++) {
+          box.lo[d] = (long long)ck[d] * per[d];
+          box.hi[d] = (long long)(ck[d] + 1) * per[d] - 1;
+        }
+        f((const Legion::IndexSpace *)&box);
+      }
+}
+
 typedef void (*SweepImpl)(const Task *, const std::vector<PhysicalRegion> &, Context, Runtime *);
 
 SweepImpl pick_sweep(int variant) {
@@ -365,14 +393,21 @@ int snapref_configure(int nx, int ny, int nz, int nang, int ng, int nmom, int tw
  * 1 center, 2 corner; src_opt: 0 everywhere, 1 center, 2 corner. */
 int snapref_configure_deck(int nx, int ny, int nz, double lx, double ly, double lz, int nang,
                            int ng, int nmom, double epsi, int iitm, int oitm, int fixup,
-                           int timedep, double tf, int nsteps, int mat_opt, int src_opt) {
+                           int timedep, double tf, int nsteps, int mat_opt, int src_opt,
+                           int ichunk, int npey, int npez) {
   if (nmom != 1) return -1;
   if (mat_opt < 0 || mat_opt > 2 || src_opt < 0 || src_opt > 3 || nsteps < 1) return -2;
+  if (ichunk < 1 || npey < 1 || npez < 1 || nx % ichunk || ny % npey || nz % npez) return -4;
   Snap::num_dims = 3;
-  Snap::nx = Snap::nx_per_chunk = nx;
-  Snap::ny = Snap::ny_per_chunk = ny;
-  Snap::nz = Snap::nz_per_chunk = nz;
-  Snap::nx_chunks = Snap::ny_chunks = Snap::nz_chunks = 1;
+  Snap::nx = nx;
+  Snap::ny = ny;
+  Snap::nz = nz;
+  Snap::nx_chunks = ichunk;   /* snap.cc:1044-1046, 1161-1163 */
+  Snap::ny_chunks = npey;
+  Snap::nz_chunks = npez;
+  Snap::nx_per_chunk = nx / ichunk;
+  Snap::ny_per_chunk = ny / npey;
+  Snap::nz_per_chunk = nz / npez;
   Snap::lx = lx;
   Snap::ly = ly;
   Snap::lz = lz;
@@ -553,15 +588,22 @@ double snapref_solve(const int32_t *mat_in, const double *qi_in, const double *s
    * per-corner angular source and, time dependent, qi = flux / v with the
    * reference flux scaled to the middle of the last step */
   if (mms) {
+    /* index launches over the chunks: each task sees its own sub-box */
     MMSInitFlux mf(snap, ref_flux, ref_fluxm);
-    execute<void>(mf, &MMSInitFlux::cpu_implementation);
+    for_each_chunk([&](const Legion::IndexSpace *b) {
+      execute<void>(mf, &MMSInitFlux::cpu_implementation, b);
+    });
     for (int i = 0; i < 8; i++) {
       MMSInitSource ms(snap, ref_flux, ref_fluxm, mat, sigt, slgg, *qim[i], i);
-      execute<void>(ms, &MMSInitSource::cpu_implementation);
+      for_each_chunk([&](const Legion::IndexSpace *b) {
+        execute<void>(ms, &MMSInitSource::cpu_implementation, b);
+      });
     }
     if (td) {
       MMSInitTimeDependent mt(snap, vel, ref_flux, qi);
-      execute<void>(mt, &MMSInitTimeDependent::cpu_implementation);
+      for_each_chunk([&](const Legion::IndexSpace *b) {
+        execute<void>(mt, &MMSInitTimeDependent::cpu_implementation, b);
+      });
     }
   }
 
@@ -578,7 +620,9 @@ double snapref_solve(const int32_t *mat_in, const double *qi_in, const double *s
     const double f = cy == 0 ? Snap::dt * 0.5 : double(2 * cy + 1) / double(2 * cy - 1);
     for (int i = 0; i < 8; i++) {
       MMSScale sc(snap, *qim[i], f);
-      execute<void>(sc, &MMSScale::cpu_implementation);
+      for_each_chunk([&](const Legion::IndexSpace *b) {
+        execute<void>(sc, &MMSScale::cpu_implementation, b);
+      });
     }
   }
   std::vector<SnapArray<3> *> &tf_in = even_time_step ? tf_even : tf_odd;
@@ -610,7 +654,27 @@ double snapref_solve(const int32_t *mat_in, const double *qi_in, const double *s
         MiniKBATask k(snap, pred, flux0, fluxm, qtot, vdelt, dinv, t_xs, *tf_in[corner],
                       *tf_out[corner], *qim[corner], flux_xy, flux_yz, flux_xz, g, g, corner,
                       ghost_offsets);
-        execute<void>(k, sweep_impl);
+        if (Snap::nx_chunks * Snap::ny_chunks * Snap::nz_chunks == 1) {
+          execute<void>(k, sweep_impl);
+          return;
+        }
+        /* one task per spatial chunk (snap.cc:56-62 blockify), upstream
+         * chunks first; chunks pass faces through the shared face arrays */
+        const int nc[3] = {Snap::nx_chunks, Snap::ny_chunks, Snap::nz_chunks};
+        const int per[3] = {Snap::nx_per_chunk, Snap::ny_per_chunk, Snap::nz_per_chunk};
+        for (int kz = 0; kz < nc[2]; kz++)
+          for (int ky = 0; ky < nc[1]; ky++)
+            for (int kx = 0; kx < nc[0]; kx++) {
+              const int ck[3] = {kx, ky, kz};
+              Legion::IndexSpace box;
+              box.dim = 3;
+              for (int d = 0; d < 3; d++) {
+                const int cc = (corner >> d) & 1 ? ck[d] : nc[d] - 1 - ck[d];
+                box.lo[d] = (long long)cc * per[d];
+                box.hi[d] = (long long)(cc + 1) * per[d] - 1;
+              }
+              execute<void>(k, sweep_impl, &box);
+            }
       });
       t_sweep += std::chrono::duration<double>(std::chrono::steady_clock::now() - ts).count();
       inners++;
@@ -641,9 +705,23 @@ double snapref_solve(const int32_t *mat_in, const double *qi_in, const double *s
   const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   if (flux_out) memcpy(flux_out, store_of(flux0).mem, C * G * sizeof(double));
   if (mms) { /* snap.cc:542-560 */
+    /* one result per chunk, folded as MMSReduction does (mms.cc:549-600):
+     * max, min, sum */
     MMSCompare cmp(snap, flux0, ref_flux);
-    const MomentTriple r = execute<MomentTriple>(cmp, &MMSCompare::cpu_implementation);
-    if (mms_out) for (int i = 0; i < 3; i++) mms_out[i] = r[i];
+    double red[3] = {0.0, 0.0, 0.0};
+    bool first = true;
+    for_each_chunk([&](const Legion::IndexSpace *b) {
+      const MomentTriple r = execute<MomentTriple>(cmp, &MMSCompare::cpu_implementation, b);
+      if (first) {
+        for (int i = 0; i < 3; i++) red[i] = r[i];
+        first = false;
+      } else {
+        red[0] = std::max(red[0], r[0]);
+        red[1] = std::min(red[1], r[1]);
+        red[2] += r[2];
+      }
+    });
+    if (mms_out) for (int i = 0; i < 3; i++) mms_out[i] = red[i];
     if (ref_flux_out) memcpy(ref_flux_out, store_of(ref_flux).mem, C * G * sizeof(double));
   }
   if (info) { info[0] = inner_total; info[1] = outer_total; info[2] = converged; }
