@@ -139,19 +139,25 @@ cudaError_t k_expand_xs(const double *sig, const int32_t *mat, double *xs, int G
 cudaError_t k_scale_xs(double *xs, const double *scale, int G, long long C, cudaStream_t st);
 cudaError_t k_expand_scat(const double *slgg, const int32_t *mat, double *s_xs, int G, int nmat,
                           int nmom, long long C, cudaStream_t st);
-cudaError_t k_outer_source(const double *qi, const double *slgg, const int32_t *mat,
-                           const double *flux, double *q2grp, int G, int nmat, int nmom, int M,
-                           long long C, cudaStream_t st);
+// outer source of output groups g_lo .. g_lo+g_n-1 from the flux of G groups:
+// the FP64 tensor-core form when `tab` (outer_dmma_table_words() doubles of
+// scratch) is given and the shape fits, else the SIMT form; *launches = the
+// kernels launched
+size_t outer_dmma_table_words(int G, int g_n, int nmat, int nmom);
 cudaError_t k_outer_source_groups(const double *qi, const double *slgg, const int32_t *mat,
-                                  const double *flux, double *q2grp, int G, int nmat, int nmom,
-                                  int M, long long C, int g_lo, int g_n, cudaStream_t st);
-// outer source with the group-to-group contraction on the BF16 tensor cores
-// (outer_tc.cu); `tab` holds outer_tc_table_words() words of scratch
+                                  const double *flux, double *q2grp, double *tab, int G, int nmat,
+                                  int nmom, int M, long long C, int g_lo, int g_n, int *launches,
+                                  cudaStream_t st);
+// outer source with the group-to-group contraction on the tcgen05 tensor
+// cores, split BF16 operands (outer_tc.cu); `tab` holds
+// outer_tc_table_words() 32-bit words of scratch; its waits record a timeout
+// in *err after timeout_ns
 size_t outer_tc_table_words(int G, int nmat, int nmom);
-size_t outer_tc_smem_bytes(int G, int nmat, int nmom);
+bool outer_tc_supported(int G, int nmat, int nmom);
 cudaError_t k_outer_source_tc(const double *qi, const double *slgg, const int32_t *mat,
                               const double *flux, double *q2grp, uint32_t *tab, int G, int nmat,
-                              int nmom, int M, long long C, cudaStream_t st);
+                              int nmom, int M, long long C, int *err, long long timeout_ns,
+                              cudaStream_t st);
 // qtot as k_inner_source, and in the same pass the old scalar flux saved to
 // old0[g*C + c] and the flux moments cleared (for sweeps that add octants
 // straight into the flux)

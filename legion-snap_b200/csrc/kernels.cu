@@ -1,5 +1,8 @@
 // HBM-bound kernels around the sweep: cross-section expansion, outer and
 // inner sources, the octant-slot reduction fused with the convergence test.
+#include <algorithm>
+
+#include "device_util.cuh"
 #include "internal.h"
 
 namespace snapb200 {
@@ -89,6 +92,137 @@ __global__ void outer_source_kernel(const double *__restrict__ qi, const double 
         acc += __ldg(row + (size_t)g2 * nmom) * sflux[(g2 * CELLS + cc) * M + m];
       }
       q2grp[((size_t)gl * C + c) * M + m] = acc;
+    }
+  }
+}
+
+// The same outer source with the group-to-group contraction on the FP64
+// tensor cores (mma.m8n8k4.f64).  For one moment k of band l the outputs of
+// 8 cells are an (output groups x 8 cells) block:
+//   D[g][c] = sum_{g'} S_l,mat(c)[g][g'] phi[g'][c][k]
+// with S the scattering matrix of band l with its diagonal zeroed (in-group
+// scattering belongs to the inner source).  Rows of D = 8 output groups per
+// MMA tile, columns = 8 cells, k = 4 input groups per MMA.  Cells of
+// different materials share one accumulator: the B operand of material m is
+// phi masked to the columns whose cell has material m, so each column
+// accumulates exactly its own material's products.
+// A warp takes a block of 8 cells and MTW output-group tiles and walks the
+// bands; per band and 4 input groups each lane loads the band's moments of
+// one (input group, cell) straight from the flux (the band's A fragment then
+// serves all of the band's moments), and writes the band's moments of its
+// (output group, 2 cells) as consecutive words.  A CTA owns one set of MTW
+// output-group tiles and keeps their fragments of every band and material
+// in shared memory (copied once from the table odm_table_kernel builds).
+constexpr int ODM_WARPS = 8;
+
+template <int NMOM, int MTW>
+size_t odm_smem_bytes(int G, int nmat) {
+  return sizeof(double) * (size_t)NMOM * nmat * MTW * ((G + 3) / 4) * 32;
+}
+
+// tab[l][m][mt][kt][lane] = S_l,m[8mt + lane/4][4kt + lane%4] (output group
+// g_lo + row, input group col), zero on the diagonal and in the padding
+__global__ void odm_table_kernel(const double *__restrict__ slgg, int G, int nmat, int nmom,
+                                 int g_lo, int g_n, int GT, int GK, double *__restrict__ tab) {
+  const long long n = (long long)nmom * nmat * GT * GK * 32;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int ln = (int)(i & 31);
+    long long r = i >> 5;
+    const int kt = (int)(r % GK);
+    r /= GK;
+    const int mt = (int)(r % GT);
+    r /= GT;
+    const int m = (int)(r % nmat);
+    const int l = (int)(r / nmat);
+    const int row = 8 * mt + (ln >> 2), col = 4 * kt + (ln & 3), go = g_lo + row;
+    tab[i] = (row < g_n && col < G && go != col)
+                 ? slgg[(((size_t)go * nmat + m) * G + col) * nmom + l]
+                 : 0.0;
+  }
+}
+
+template <int NMOM, int MTW>
+__global__ void __launch_bounds__(ODM_WARPS * 32)
+    outer_source_dmma_kernel(const double *__restrict__ qi, const double *__restrict__ tab,
+                             const int32_t *__restrict__ mat, const double *__restrict__ flux,
+                             double *__restrict__ q2grp, int G, int nmat, long long C, int g_n,
+                             int GT, int n_mg) {
+  constexpr int M = NMOM * NMOM, NKMAX = 2 * NMOM - 1;
+  extern __shared__ __align__(16) double odm_smem[];   // [l][mat][j][kt][32]
+  const int GK = (G + 3) / 4;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int mg = blockIdx.x % n_mg, p = blockIdx.x / n_mg, P = gridDim.x / n_mg;
+  // this CTA's fragments: output-group tiles mg*MTW + j of every band and material
+  for (int i = tid; i < NMOM * nmat * MTW * GK * 32; i += blockDim.x) {
+    const int ln = i & 31, kt = (i >> 5) % GK, j = (i >> 5) / GK % MTW, lm = (i >> 5) / (GK * MTW);
+    const int mt = mg * MTW + j;
+    odm_smem[i] = mt < GT ? __ldg(tab + (((size_t)lm * GT + mt) * GK + kt) * 32 + ln) : 0.0;
+  }
+  __syncthreads();
+  const long long nblocks = (C + 7) / 8;
+  for (long long blk = (long long)p * ODM_WARPS + w; blk < nblocks; blk += (long long)P * ODM_WARPS) {
+    // B column of this lane: cell blk*8 + lane/4, input group 4kt + lane%4
+    const long long cb = blk * 8 + (lane >> 2);
+    const int matb = cb < C ? mat[cb] - 1 : -1;
+#pragma unroll
+    for (int l = 0; l < NMOM; ++l) {
+      const int k0 = l * l, nk = 2 * l + 1;
+      double acc[MTW][NKMAX][2];
+#pragma unroll
+      for (int j = 0; j < MTW; ++j)
+#pragma unroll
+        for (int kk = 0; kk < NKMAX; ++kk) acc[j][kk][0] = acc[j][kk][1] = 0.0;
+      // the band's moments of (input group 4kt + lane%4, cell cb), one
+      // input-group step ahead of the MMAs that use them
+      double bn[NKMAX];
+      auto load_b = [&](int kt) {
+        const int gb = 4 * kt + (lane & 3);
+        const bool in = kt < GK && gb < G && cb < C;
+        const double *src = flux + ((size_t)(in ? gb : 0) * C + (in ? cb : 0)) * M + k0;
+#pragma unroll
+        for (int kk = 0; kk < NKMAX; ++kk) bn[kk] = (kk < nk && in) ? __ldg(src + kk) : 0.0;
+      };
+      load_b(0);
+      for (int kt = 0; kt < GK; ++kt) {
+        double b[NKMAX];
+#pragma unroll
+        for (int kk = 0; kk < NKMAX; ++kk) b[kk] = bn[kk];
+        load_b(kt + 1);
+        for (int m = 0; m < nmat; ++m) {
+          const double *a = odm_smem + ((size_t)(l * nmat + m) * MTW * GK + kt) * 32 + lane;
+          const bool mine = matb == m;
+          double bm[NKMAX];
+#pragma unroll
+          for (int kk = 0; kk < NKMAX; ++kk) bm[kk] = mine ? b[kk] : 0.0;
+#pragma unroll
+          for (int j = 0; j < MTW; ++j) {
+            const double aj = a[(size_t)j * GK * 32];
+#pragma unroll
+            for (int kk = 0; kk < NKMAX; ++kk)
+              if (kk < nk) dmma_8x8x4(acc[j][kk][0], acc[j][kk][1], aj, bm[kk]);
+          }
+        }
+      }
+      // D rows (output groups) 8mt + lane/4, columns (cells) 2(lane%4) + {0,1}
+#pragma unroll
+      for (int j = 0; j < MTW; ++j) {
+        const int gl = 8 * (mg * MTW + j) + (lane >> 2);
+        if (gl >= g_n) continue;
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const long long c = blk * 8 + 2 * (lane & 3) + e;
+          if (c >= C) continue;
+          double *dst = q2grp + ((size_t)gl * C + c) * M + k0;
+#pragma unroll
+          for (int kk = 0; kk < NKMAX; ++kk) {
+            if (kk >= nk) continue;
+            double v = acc[j][kk][e];
+            if (l == 0) v += qi[(size_t)gl * C + c];
+            dst[kk] = v;
+          }
+        }
+      }
     }
   }
 }
@@ -457,15 +591,70 @@ cudaError_t k_expand_scat(const double *slgg, const int32_t *mat, double *s_xs, 
   return cudaGetLastError();
 }
 
-cudaError_t k_outer_source(const double *qi, const double *slgg, const int32_t *mat,
-                           const double *flux, double *q2grp, int G, int nmat, int nmom, int M,
-                           long long C, cudaStream_t st) {
-  return k_outer_source_groups(qi, slgg, mat, flux, q2grp, G, nmat, nmom, M, C, 0, G, st);
+namespace {
+
+template <int NMOM, int MTW>
+cudaError_t launch_outer_dmma(const double *qi, const double *tab, const int32_t *mat,
+                              const double *flux, double *q2grp, int G, int nmat, long long C,
+                              int g_n, cudaStream_t st) {
+  auto kern = outer_source_dmma_kernel<NMOM, MTW>;
+  const size_t smem = odm_smem_bytes<NMOM, MTW>(G, nmat);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 0, blocks = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kern, ODM_WARPS * 32, smem)) !=
+      cudaSuccess)
+    return e;
+  const int GT = (g_n + 7) / 8, n_mg = (GT + MTW - 1) / MTW;
+  // CTAs per output-group set: fill the device, at most one warp per cell block
+  const long long nblocks = (C + 7) / 8;
+  const long long per_set =
+      std::max<long long>(1, std::min<long long>((long long)std::max(blocks, 1) * sms / n_mg,
+                                                 (nblocks + ODM_WARPS - 1) / ODM_WARPS));
+  kern<<<(int)(per_set * n_mg), ODM_WARPS * 32, smem, st>>>(qi, tab, mat, flux, q2grp, G, nmat, C,
+                                                            g_n, GT, n_mg);
+  return cudaGetLastError();
+}
+
+template <int NMOM>
+cudaError_t launch_outer_dmma_mtw(const double *qi, const double *tab, const int32_t *mat,
+                                  const double *flux, double *q2grp, int G, int nmat, long long C,
+                                  int g_n, cudaStream_t st) {
+  const int GT = (g_n + 7) / 8;
+  if (GT == 1) return launch_outer_dmma<NMOM, 1>(qi, tab, mat, flux, q2grp, G, nmat, C, g_n, st);
+  if (GT == 2) return launch_outer_dmma<NMOM, 2>(qi, tab, mat, flux, q2grp, G, nmat, C, g_n, st);
+  return launch_outer_dmma<NMOM, 4>(qi, tab, mat, flux, q2grp, G, nmat, C, g_n, st);
+}
+
+}  // namespace
+
+size_t outer_dmma_table_words(int G, int g_n, int nmat, int nmom) {
+  return (size_t)nmom * nmat * ((g_n + 7) / 8) * ((G + 3) / 4) * 32;
 }
 
 cudaError_t k_outer_source_groups(const double *qi, const double *slgg, const int32_t *mat,
-                                  const double *flux, double *q2grp, int G, int nmat, int nmom,
-                                  int M, long long C, int g_lo, int g_n, cudaStream_t st) {
+                                  const double *flux, double *q2grp, double *tab, int G, int nmat,
+                                  int nmom, int M, long long C, int g_lo, int g_n, int *launches,
+                                  cudaStream_t st) {
+  *launches = 1;
+  // tensor-core form when its fragments fit in shared memory
+  const int GT = (g_n + 7) / 8, GK = (G + 3) / 4;
+  const size_t dsmem = sizeof(double) * (size_t)nmom * nmat * std::min(GT, 4) * GK * 32;
+  if (tab && dsmem <= 160 * 1024) {
+    *launches = 2;
+    odm_table_kernel<<<32, 256, 0, st>>>(slgg, G, nmat, nmom, g_lo, g_n, GT, GK, tab);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    switch (nmom) {
+      case 1: return launch_outer_dmma_mtw<1>(qi, tab, mat, flux, q2grp, G, nmat, C, g_n, st);
+      case 2: return launch_outer_dmma_mtw<2>(qi, tab, mat, flux, q2grp, G, nmat, C, g_n, st);
+      case 3: return launch_outer_dmma_mtw<3>(qi, tab, mat, flux, q2grp, G, nmat, C, g_n, st);
+      case 4: return launch_outer_dmma_mtw<4>(qi, tab, mat, flux, q2grp, G, nmat, C, g_n, st);
+      default: *launches = 1; break;
+    }
+  }
   constexpr int CELLS = 4;
   const size_t smem = sizeof(double) * G * CELLS * M;
   if (smem > 200 * 1024) return cudaErrorInvalidValue;

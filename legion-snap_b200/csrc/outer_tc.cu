@@ -1,214 +1,420 @@
-// Outer source with the group-to-group scattering contraction on the BF16
-// tensor cores (the precision form's fast outer source).
+// Outer source with the group-to-group scattering contraction on the
+// fifth-generation tensor cores (tcgen05.mma, kind::f16: BF16 operands, FP32
+// accumulation in tensor memory) -- the precision form's fast outer source.
 //
-// Same result as outer_source_kernel (kernels.cu; reference: CalcOuterSource,
-// outer.cc:107-217, gpu_outer.cu:76-441):
+// Same result as the FP64 outer source (kernels.cu; reference:
+// CalcOuterSource, outer.cc:107-217, gpu_outer.cu:76-441):
 //   q2[g][c][k] = qi[g][c] [k = 0] + sum_{g' != g} slgg[g][mat(c)][g'][l(k)] phi[g'][c][k]
-// For a fixed moment k (hence band l) and material, this is a GEMM of the
-// G x G scattering block with the G x cells flux block; it runs on
-// mma.m16n8k16 with the output groups as rows, the input groups as k and 8
-// cells as columns.  BF16 keeps 8 mantissa bits, so both operands are split
-// x = hi + lo (hi the BF16 rounding of x, lo that of the remainder) and the
-// product is accumulated as lo*hi + hi*lo + hi*hi in FP32: relative error of
-// order 2^-16.  That is not the FP64 source: the solve driver uses this only
-// while the outer iteration is still far from converged and switches to the
-// FP64 source for the final outer iterations (a mixed-precision refinement:
-// the converged fixed point is the one of the FP64 source).
+// For one moment k (hence band l) and 128 cells this is a GEMM
+//   D[c][g] = sum_{g'} A[c][g'] B[g][g'],   A = phi[.][c][k], B = S_l,mat
+// with the cells as the MMA's M = 128 rows (tensor-memory lanes), the output
+// groups as N and the input groups as K.  BF16 keeps 8 mantissa bits, so
+// both operands are split x = hi + lo (hi the BF16 rounding of x, lo that of
+// the remainder) and the product is accumulated as hi*hi + hi*lo + lo*hi:
+// relative error of order 2^-16.  That is not the FP64 source: the solve
+// driver uses this only while the outer iteration is still far from
+// converged and switches to the FP64 source for the final outer iterations
+// (a mixed-precision refinement: the converged fixed point is the one of the
+// FP64 source).  Cells of different materials: the A operand is staged once
+// per material with the rows of other materials zeroed, and the materials'
+// products accumulate into the same tensor-memory tile.
 //
-// A CTA takes 32 cells (4 warps x 8) and walks the moment bands: for band l
-// it stages the split scattering blocks of every material (MMA fragment
-// layout, built once per call by tc_tables_kernel) and the split flux of the
-// band's moments (input group fastest) in shared memory, then each warp forms
-// its 8 cells x all output groups for each moment of the band.  A cell tile
-// holding several materials computes each present material and selects per
-// column.
+// Operands live in shared memory in the K-major layout without swizzle:
+// 8-row x 16-byte core matrices, the two core matrices of one 16-element K
+// step 128 bytes apart (leading byte offset), consecutive 8-row groups 256
+// bytes apart (stride byte offset), K steps one after another.  The
+// scattering operands of every band and material (built per call by
+// tcb_table_kernel in that layout) are copied into shared memory once per
+// CTA with one bulk copy (cp.async.bulk, completion on an mbarrier).  Per
+// moment the 128 threads convert their cell's flux to the split operands,
+// one elected thread issues the MMAs and commits them to an mbarrier, and
+// every MC moments the four warps read their 32 lanes of the accumulators
+// back (tcgen05.ld) and store the MC consecutive moments of each (group,
+// cell) as one 32-byte run.  Every wait is bounded and records a timeout in
+// the device error word.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 
+#include "device_util.cuh"
 #include "internal.h"
 
 namespace snapb200 {
 namespace {
 
-constexpr int TCELLS = 32;   // cells per CTA (4 warps x 8)
+constexpr int TCR = 128;   // cells per tile = MMA rows; 4 warps, warp w owns lanes 32w..32w+31
+constexpr int MCMAX = 4;   // moments per accumulator batch
 
+__host__ __device__ inline int pad16(int x) { return (x + 15) / 16 * 16; }
 
-// two BF16 values packed low (first) / high (second)
-__device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 lo_half, __nv_bfloat16 hi_half) {
-  return (uint32_t)__bfloat16_as_ushort(lo_half) | ((uint32_t)__bfloat16_as_ushort(hi_half) << 16);
+// Byte offset of element (row r, k) of a K-major BF16 operand tile of R rows.
+__host__ __device__ inline uint32_t kmajor_offset(int R, int r, int k) {
+  return (uint32_t)((k >> 4) * (R / 8) * 256 + (r >> 3) * 256 + ((k >> 3) & 1) * 128 +
+                    (r & 7) * 16 + (k & 7) * 2);
 }
-// split x = hi + lo, both BF16 rounded to nearest
+
+// Shared-memory matrix descriptor: start address, leading byte offset 128,
+// stride byte offset 256, descriptor version 1, no swizzle.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) |
+         ((uint64_t)(256 >> 4) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both
+// K-major, N columns, M = 128 rows.
+__host__ __device__ inline uint32_t idesc_bf16(int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(TCR >> 4) << 24);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+// Waits until the phase with parity `parity` of the mbarrier has completed.
+// Gives up after timeout_ns of device time or an iteration cap (recording a
+// timeout), or when the device error word is set.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int *err,
+                                          long long timeout_ns) {
+  const long long t0 = global_timer_ns();
+  for (unsigned spins = 0;; ++spins) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if ((spins & 63u) == 63u) {
+      if (ld_volatile(err) != 0) return false;
+      if (global_timer_ns() - t0 > timeout_ns || spins > (1u << 24)) {
+        atomicCAS(err, 0, DEV_ERR_TIMEOUT);
+        return false;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void fence_before_sync() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_after_sync() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// D[tmem] (+)= A * B^T, M = 128, K = 16, one elected thread.
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+// Arrives on the mbarrier once every MMA this thread issued so far is done.
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+               : "memory");
+}
+
+// 16 consecutive FP32 accumulator columns of this thread's lane.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+      "%12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tmem_wait_ld() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
 __device__ __forceinline__ void split_bf16(double x, __nv_bfloat16 &hi, __nv_bfloat16 &lo) {
   hi = __double2bfloat16(x);
   lo = __double2bfloat16(x - (double)__bfloat162float(hi));
 }
 
-// Scattering blocks in the A-fragment layout of mma.m16n8k16 (row-major
-// A[row = output group][col = input group]); lane l = 4r + t holds
-// reg 0 = A[r][2t, 2t+1], reg 1 = A[r+8][2t, 2t+1], reg 2 = A[r][2t+8, 2t+9],
-// reg 3 = A[r+8][2t+8, 2t+9].  Table [l][mat][mt][kt][lane][8]: regs 0-3 hi,
-// 4-7 lo.  The diagonal (in-group scattering, handled by the inner source)
-// and the padding beyond G are zero.
-__global__ void tc_tables_kernel(const double *__restrict__ slgg, int G, int nmat, int nmom,
-                                 int GT, uint32_t *__restrict__ tab) {
-  const long long n = (long long)nmom * nmat * GT * GT * 32 * 4;
+// Scattering operands B[g][g'] = S_l,mat[g][g'] (diagonal and padding zero),
+// split into BF16 hi and lo, each an N x KP tile in the K-major layout;
+// order [l][mat][part].
+__global__ void tcb_table_kernel(const double *__restrict__ slgg, int G, int nmat, int nmom, int N,
+                                 int KP, __nv_bfloat16 *__restrict__ tab) {
+  const long long per = (long long)N * KP;
+  const long long n = (long long)nmom * nmat * per;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
-    const int reg = (int)(i % 4), lane = (int)((i / 4) % 32);
-    long long rest = i / 128;
-    const int kt = (int)(rest % GT);
-    rest /= GT;
-    const int mt = (int)(rest % GT);
-    rest /= GT;
-    const int m = (int)(rest % nmat);
-    const int l = (int)(rest / nmat);
-    const int r = lane >> 2, t = lane & 3;
-    const int row = 16 * mt + r + ((reg & 1) ? 8 : 0);
-    const int col = 16 * kt + 2 * t + ((reg & 2) ? 8 : 0);
-    __nv_bfloat16 h[2], lo[2];
-    for (int e = 0; e < 2; ++e) {
-      const int c = col + e;
-      const double v = (row < G && c < G && row != c)
-                           ? slgg[(((size_t)row * nmat + m) * G + c) * nmom + l]
-                           : 0.0;
-      split_bf16(v, h[e], lo[e]);
-    }
-    uint32_t *dst = tab + (i / 4) * 8;
-    dst[reg] = pack_bf16(h[0], h[1]);
-    dst[4 + reg] = pack_bf16(lo[0], lo[1]);
+    const int k = (int)(i % KP), row = (int)((i / KP) % N);
+    const long long lm = i / per;
+    const int m = (int)(lm % nmat), l = (int)(lm / nmat);
+    const double v = (row < G && k < G && row != k)
+                         ? slgg[(((size_t)row * nmat + m) * G + k) * nmom + l]
+                         : 0.0;
+    __nv_bfloat16 h, lo;
+    split_bf16(v, h, lo);
+    __nv_bfloat16 *tile = tab + (size_t)lm * 2 * per;
+    const uint32_t off = kmajor_offset(N, row, k) / 2;
+    tile[off] = h;
+    tile[per + off] = lo;
   }
 }
 
-__device__ __forceinline__ void mma_bf16(float (&d)[4], uint4 a, uint32_t b0, uint32_t b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
-      "{%8,%9}, {%0,%1,%2,%3};\n"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a.x), "r"(a.y), "r"(a.z), "r"(a.w), "r"(b0), "r"(b1));
-}
-
-// Dynamic shared memory: fragments [nmat][GT][GT][32] x 2 uint4 (hi, lo),
-// then the band's split flux, hi and lo, each [2*nmom-1][TCELLS][PG] BF16
-// with PG = 16*GT + 8 (the pad spreads the 8 cells of a fragment load over
-// all banks).
-__global__ void __launch_bounds__(128)
-    outer_source_tc_kernel(const double *__restrict__ qi, const uint32_t *__restrict__ tab,
+__global__ void __launch_bounds__(TCR)
+    outer_source_tc_kernel(const double *__restrict__ qi, const __nv_bfloat16 *__restrict__ tab,
                            const int32_t *__restrict__ mat, const double *__restrict__ flux,
-                           double *__restrict__ q2grp, int G, int nmat, int nmom, int M,
-                           long long C, int GT) {
-  extern __shared__ __align__(16) uint4 smem_u4[];
-  const int PG = 16 * GT + 8;
-  const int KMAX = 2 * nmom - 1;
-  uint4 *sA = smem_u4;                                        // [nmat][GT][GT][32][2]
-  __nv_bfloat16 *sPh = (__nv_bfloat16 *)(sA + (size_t)nmat * GT * GT * 64);
-  __nv_bfloat16 *sPl = sPh + (size_t)KMAX * TCELLS * PG;
-  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  const int r = lane >> 2, t = lane & 3;
-  const long long ntiles = (C + TCELLS - 1) / TCELLS;
+                           double *__restrict__ q2grp, int G, int N, int KP, int nmat, int nmom,
+                           int M, int MC, long long C, int tmem_cols, int *err,
+                           long long timeout_ns) {
+  extern __shared__ __align__(1024) unsigned char tc_smem[];
+  const size_t b_tile = (size_t)N * KP * 2, a_tile = (size_t)TCR * KP * 2;
+  const size_t b_bytes = (size_t)nmom * nmat * 2 * b_tile;
+  unsigned char *sB = tc_smem;                 // [l][mat][hi, lo] N x KP
+  unsigned char *sA = tc_smem + b_bytes;       // [moment of the batch][hi, lo] 128 x KP
+  __shared__ __align__(8) uint64_t s_bar[2];   // 0: table copy, 1: MMA completion
+  __shared__ uint32_t s_tmem;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const uint32_t bar_tab = smem_u32(&s_bar[0]), bar_mma = smem_u32(&s_bar[1]);
+  const uint32_t idesc = idesc_bf16(N);
 
-  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const long long c0 = tile * TCELLS;
-    // this lane's output columns: cells 8w + 2t, 8w + 2t + 1 of the tile
-    const long long ca = c0 + 8 * w + 2 * t, cb = ca + 1;
-    const int mata = ca < C ? mat[ca] - 1 : -1, matb = cb < C ? mat[cb] - 1 : -1;
-    // materials present in the warp's 8 cells (lanes 0-7 look at one cell each)
-    const long long cm = c0 + 8 * w + (lane & 7);
-    const unsigned present = __reduce_or_sync(0xffffffffu, (lane < 8 && cm < C) ? 1u << (mat[cm] - 1) : 0u);
-    for (int l = 0; l < nmom; ++l) {
-      const int k0 = l * l, nk = 2 * l + 1;
-      __syncthreads();
-      // stage the scattering fragments of band l and the band's split flux
-      const uint4 *src = (const uint4 *)(tab + (size_t)l * nmat * GT * GT * 32 * 8);
-      for (int i = tid; i < nmat * GT * GT * 64; i += blockDim.x) sA[i] = src[i];
-      // (moment fastest, then cell: neighbouring threads read neighbouring words)
-      for (int i = tid; i < nk * TCELLS * 16 * GT; i += blockDim.x) {
-        const int kk = i % nk, cc = (i / nk) % TCELLS, g = i / (nk * TCELLS);
-        const long long c = c0 + cc;
-        const double v = (g < G && c < C) ? flux[((size_t)g * C + c) * M + k0 + kk] : 0.0;
-        __nv_bfloat16 h, lo;
-        split_bf16(v, h, lo);
-        const size_t at = ((size_t)kk * TCELLS + cc) * PG + g;
-        sPh[at] = h;
-        sPl[at] = lo;
-      }
-      __syncthreads();
-      for (int kk = 0; kk < nk; ++kk) {
-        const int k = k0 + kk;
-        // B fragments: rows = input groups 16kt + 2t (+1, +8, +9), column = cell 8w + r
-        const __nv_bfloat16 *bh = sPh + ((size_t)kk * TCELLS + 8 * w + r) * PG + 2 * t;
-        const __nv_bfloat16 *bl = sPl + ((size_t)kk * TCELLS + 8 * w + r) * PG + 2 * t;
-        for (int mt = 0; mt < GT; ++mt) {
-          float out[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-          for (int m = 0; m < nmat; ++m) {
-            if (!((present >> m) & 1u)) continue;
-            float d[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-            for (int kt = 0; kt < GT; ++kt) {
-              const uint4 *a = sA + ((((size_t)m * GT + mt) * GT + kt) * 32 + lane) * 2;
-              const uint4 ah = a[0], al = a[1];
-              const uint32_t bh0 = *(const uint32_t *)(bh + 16 * kt);
-              const uint32_t bh1 = *(const uint32_t *)(bh + 16 * kt + 8);
-              const uint32_t bl0 = *(const uint32_t *)(bl + 16 * kt);
-              const uint32_t bl1 = *(const uint32_t *)(bl + 16 * kt + 8);
-              mma_bf16(d, al, bh0, bh1);
-              mma_bf16(d, ah, bl0, bl1);
-              mma_bf16(d, ah, bh0, bh1);
-            }
-            if (mata == m) { out[0] = d[0]; out[2] = d[2]; }
-            if (matb == m) { out[1] = d[1]; out[3] = d[3]; }
+  if (tid == 0) {
+    mbar_init(bar_tab, 1);
+    mbar_init(bar_mma, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&s_tmem)),
+                 "r"(tmem_cols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const uint32_t tmem = s_tmem;
+  // the scattering operands of every band and material: bulk copies
+  if (tid == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_tab),
+                 "r"((uint32_t)b_bytes)
+                 : "memory");
+    for (size_t off = 0; off < b_bytes; off += 16384) {
+      const uint32_t len = (uint32_t)(b_bytes - off < 16384 ? b_bytes - off : 16384);
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+              smem_u32(sB + off)),
+          "l"((const unsigned char *)tab + off), "r"(len), "r"(bar_tab)
+          : "memory");
+    }
+  }
+  // (every wait's outcome is made CTA-uniform before anyone acts on it, so
+  // that all threads meet the same barriers)
+  bool ok = __syncthreads_and(tid != 0 || mbar_wait(bar_tab, 0, err, timeout_ns));
+
+  uint32_t commits = 0;
+  const long long ntiles = (C + TCR - 1) / TCR;
+  const bool runs4 = (M & 3) == 0;   // a batch of 4 moments is one aligned 32-byte run
+  for (long long tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x) {
+    const long long c = tile * TCR + tid;   // this thread's cell = A row = accumulator lane
+    const bool valid = c < C;
+    const int matr = valid ? mat[c] - 1 : -1;
+    for (int m0 = 0; ok && m0 < M; m0 += MC) {
+      const int mc = min(MC, M - m0);
+      // the batch's split flux: each (input group, cell) run of mc moments is
+      // read once and converted into row tid of the batch's A operands
+      for (int k8 = 0; k8 < KP; k8 += 8) {
+        double x[8][MCMAX];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          const int gi = k8 + e;
+          const double *src = flux + ((size_t)gi * C + c) * M + m0;
+          if (valid && gi < G && mc == 4 && runs4) {
+            const double2 v0 = __ldg((const double2 *)src), v1 = __ldg((const double2 *)src + 1);
+            x[e][0] = v0.x;
+            x[e][1] = v0.y;
+            x[e][2] = v1.x;
+            x[e][3] = v1.y;
+          } else {
+#pragma unroll
+            for (int mm = 0; mm < MCMAX; ++mm)
+              x[e][mm] = (valid && gi < G && mm < mc) ? __ldg(src + mm) : 0.0;
           }
-          // rows 16mt + r and 16mt + r + 8 (output groups), columns ca, cb
-          const int g_a = 16 * mt + r, g_b = g_a + 8;
-          auto put = [&](int g, long long c, float v) {
-            if (g >= G || c >= C) return;
-            double q = (double)v;
-            if (k == 0) q += qi[(size_t)g * C + c];
-            q2grp[((size_t)g * C + c) * M + k] = q;
-          };
-          put(g_a, ca, out[0]);
-          put(g_a, cb, out[1]);
-          put(g_b, ca, out[2]);
-          put(g_b, cb, out[3]);
+        }
+        const uint32_t off = kmajor_offset(TCR, tid, k8);
+#pragma unroll
+        for (int mm = 0; mm < MCMAX; ++mm) {
+          if (mm >= mc) break;
+          __align__(16) __nv_bfloat16 h[8], lo[8];
+#pragma unroll
+          for (int e = 0; e < 8; ++e) split_bf16(x[e][mm], h[e], lo[e]);
+          unsigned char *t = sA + (size_t)mm * 2 * a_tile;
+          *(uint4 *)(t + off) = *(const uint4 *)h;
+          *(uint4 *)(t + a_tile + off) = *(const uint4 *)lo;
         }
       }
+      // make the operands visible to the tensor cores, then one thread issues:
+      // moment mm, material mi -> accumulator columns (mm * nmat + mi) * N
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncthreads();
+      if (tid == 0) {
+        fence_after_sync();
+        for (int mm = 0; mm < mc; ++mm) {
+          const int k = m0 + mm;
+          int l = 0;
+          while ((l + 1) * (l + 1) <= k) ++l;
+          const uint32_t a_hi = smem_u32(sA + (size_t)mm * 2 * a_tile), a_lo = a_hi + (uint32_t)a_tile;
+          for (int mi = 0; mi < nmat; ++mi) {
+            const uint32_t d = tmem + (uint32_t)((mm * nmat + mi) * N);
+            const uint32_t b_hi = smem_u32(sB + ((size_t)l * nmat + mi) * 2 * b_tile),
+                           b_lo = b_hi + (uint32_t)b_tile;
+            for (int s = 0; s < KP / 16; ++s) {
+              const uint32_t ao = (uint32_t)s * (TCR / 8) * 256, bo = (uint32_t)s * (N / 8) * 256;
+              mma_bf16(d, smem_desc(a_hi + ao), smem_desc(b_hi + bo), idesc, s > 0);
+              mma_bf16(d, smem_desc(a_hi + ao), smem_desc(b_lo + bo), idesc, 1);
+              mma_bf16(d, smem_desc(a_lo + ao), smem_desc(b_hi + bo), idesc, 1);
+            }
+          }
+        }
+        mma_commit(bar_mma);
+      }
+      ++commits;
+      // accumulators of the batch: wait, read this thread's lane (its cell's
+      // material), store
+      ok = __syncthreads_and(mbar_wait(bar_mma, (commits - 1) & 1u, err, timeout_ns));
+      if (!ok) break;
+      fence_after_sync();
+      const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+      for (int gb = 0; gb < N; gb += 16) {
+        float v[MCMAX][16];
+#pragma unroll
+        for (int mm = 0; mm < MCMAX; ++mm) {
+          if (mm >= mc) break;
+          for (int mi = 0; mi < nmat; ++mi) {
+            float t[16];
+            tmem_ld16(lane_addr + (uint32_t)((mm * nmat + mi) * N + gb), t);
+            tmem_wait_ld();
+            if (mi == matr) {
+#pragma unroll
+              for (int j = 0; j < 16; ++j) v[mm][j] = t[j];
+            }
+          }
+        }
+        if (!valid) continue;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int g = gb + j;
+          if (g >= G) break;
+          double o[MCMAX];
+#pragma unroll
+          for (int mm = 0; mm < MCMAX; ++mm) o[mm] = mm < mc ? (double)v[mm][j] : 0.0;
+          if (m0 == 0) o[0] += qi[(size_t)g * C + c];
+          double *dst = q2grp + ((size_t)g * C + c) * M + m0;
+          if (mc == 4 && runs4) {
+            *(double2 *)dst = make_double2(o[0], o[1]);
+            *(double2 *)(dst + 2) = make_double2(o[2], o[3]);
+          } else {
+#pragma unroll
+            for (int mm = 0; mm < MCMAX; ++mm)
+              if (mm < mc) dst[mm] = o[mm];
+          }
+        }
+      }
+      // the next batch overwrites the A operands and the accumulators
+      fence_before_sync();
+      __syncthreads();
     }
   }
+  fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    fence_after_sync();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols)
+                 : "memory");
+  }
+}
+
+// Launch plan: moments per batch MC (the largest of 4, 2, 1 whose
+// accumulators, MC * nmat tiles of N columns, fit the 512 tensor-memory
+// columns and whose operands fit 200 KB of shared memory), the tensor-memory
+// columns to allocate (a power of two >= 32) and the shared-memory bytes.
+struct TcPlan {
+  int N, KP, MC, cols;
+  size_t smem;
+};
+
+bool tc_plan(int G, int nmat, int nmom, TcPlan *pl) {
+  pl->N = pad16(G);
+  pl->KP = pad16(G);
+  const size_t b_bytes = (size_t)nmom * nmat * 2 * pl->N * pl->KP * 2;
+  for (int mc = MCMAX; mc >= 1; mc /= 2) {
+    const size_t smem = b_bytes + (size_t)mc * 2 * TCR * pl->KP * 2;
+    if ((long long)mc * nmat * pl->N <= 512 && smem <= 200 * 1024) {
+      pl->MC = mc;
+      pl->smem = smem;
+      pl->cols = 32;
+      while (pl->cols < mc * nmat * pl->N) pl->cols <<= 1;
+      return true;
+    }
+  }
+  return false;
 }
 
 }  // namespace
 
 size_t outer_tc_table_words(int G, int nmat, int nmom) {
-  const int GT = (G + 15) / 16;
-  return (size_t)nmom * nmat * GT * GT * 32 * 8;
+  // BF16 words, counted in 32-bit units
+  return (size_t)nmom * nmat * 2 * pad16(G) * pad16(G) / 2;
 }
 
-size_t outer_tc_smem_bytes(int G, int nmat, int nmom) {
-  const int GT = (G + 15) / 16, PG = 16 * GT + 8;
-  return sizeof(uint4) * (size_t)nmat * GT * GT * 64 +
-         2 * sizeof(__nv_bfloat16) * (size_t)(2 * nmom - 1) * TCELLS * PG;
+bool outer_tc_supported(int G, int nmat, int nmom) {
+  TcPlan pl;
+  return tc_plan(G, nmat, nmom, &pl);
 }
 
 cudaError_t k_outer_source_tc(const double *qi, const double *slgg, const int32_t *mat,
                               const double *flux, double *q2grp, uint32_t *tab, int G, int nmat,
-                              int nmom, int M, long long C, cudaStream_t st) {
-  const int GT = (G + 15) / 16;
-  const size_t smem = outer_tc_smem_bytes(G, nmat, nmom);
-  if (smem > 200 * 1024 || nmat > 32) return cudaErrorInvalidValue;
-  tc_tables_kernel<<<64, 256, 0, st>>>(slgg, G, nmat, nmom, GT, tab);
+                              int nmom, int M, long long C, int *err, long long timeout_ns,
+                              cudaStream_t st) {
+  TcPlan pl;
+  if (!tc_plan(G, nmat, nmom, &pl)) return cudaErrorInvalidValue;
+  tcb_table_kernel<<<64, 256, 0, st>>>(slgg, G, nmat, nmom, pl.N, pl.KP, (__nv_bfloat16 *)tab);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(outer_source_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem);
+                           (int)pl.smem);
   if (e != cudaSuccess) return e;
-  int dev = 0, sms = 0, blocks = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, outer_source_tc_kernel, 128, smem);
-  const long long tiles = (C + TCELLS - 1) / TCELLS;
-  const int grid = (int)std::min<long long>(tiles, (long long)std::max(blocks, 1) * sms);
-  outer_source_tc_kernel<<<grid, 128, smem, st>>>(qi, tab, mat, flux, q2grp, G, nmat, nmom, M, C,
-                                                  GT);
+  e = cudaFuncSetAttribute(outer_source_tc_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           (int)cudaSharedmemCarveoutMaxShared);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 0, smem_sm = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) !=
+      cudaSuccess)
+    return e;
+  cudaFuncAttributes fa;
+  if ((e = cudaFuncGetAttributes(&fa, outer_source_tc_kernel)) != cudaSuccess) return e;
+  // resident CTAs: by shared memory (with the static part and the per-CTA
+  // reserve), by the 512 tensor-memory columns, by registers
+  const int by_smem = (int)((size_t)smem_sm / (pl.smem + 2048));
+  const int by_regs = 65536 / (((fa.numRegs + 7) / 8 * 8) * TCR);
+  const int blocks = std::max(1, std::min(std::min(by_smem, 512 / pl.cols), by_regs));
+  const long long tiles = (C + TCR - 1) / TCR;
+  const int grid = (int)std::min<long long>(tiles, (long long)blocks * sms);
+  outer_source_tc_kernel<<<grid, TCR, pl.smem, st>>>(qi, (const __nv_bfloat16 *)tab, mat, flux,
+                                                     q2grp, G, pl.N, pl.KP, nmat, nmom, M, pl.MC,
+                                                     C, pl.cols, err, timeout_ns);
   return cudaGetLastError();
 }
 

@@ -68,6 +68,8 @@ struct snap_ctx {
   int *d_pair_table = nullptr, *d_pair_index = nullptr;
   void *d_tc1 = nullptr, *d_tc2 = nullptr;
   uint32_t *d_scat_tc = nullptr;   // BF16 scattering fragments of the tensor-core outer source
+  double *d_odm_tab = nullptr;     // FP64 scattering fragments of the outer source
+  size_t odm_tab_words = 0;
   double *d_old0 = nullptr;        // [G][C] scalar flux before the current inner sweep
   bool atomic_octants = true;      // inner iterations add octants straight into the flux
   void *d_slots = nullptr, *d_bx = nullptr, *d_by = nullptr;
@@ -133,6 +135,7 @@ void free_ctx(snap_ctx *c) {
   cudaFree(c->d_tc1);
   cudaFree(c->d_tc2);
   cudaFree(c->d_scat_tc);
+  cudaFree(c->d_odm_tab);
   cudaFree(c->d_old0);
   cudaFree(c->d_slots);
   cudaFree(c->d_bx);
@@ -517,6 +520,30 @@ extern "C" {
 
 const char *snap_last_error(void) { return g_last_error.c_str(); }
 
+// The outer source of output groups g_lo .. g_lo+g_n-1 from the flux of G
+// groups (kernels.cu: FP64 tensor-core form with its fragment table in
+// d_odm_tab, grown on demand; the SIMT form when the table cannot be had).
+cudaError_t outer_source(snap_ctx *c, const double *qi, const double *slgg, const int32_t *mat,
+                         const double *flux, double *q2, int G, int g_lo, int g_n,
+                         cudaStream_t st) {
+  const size_t words = outer_dmma_table_words(G, g_n, c->cfg.nmat, c->cfg.nmom);
+  if (words > c->odm_tab_words) {
+    cudaFree(c->d_odm_tab);
+    c->d_odm_tab = nullptr;
+    c->odm_tab_words = 0;
+    if (cudaMalloc((void **)&c->d_odm_tab, sizeof(double) * words) == cudaSuccess)
+      c->odm_tab_words = words;
+    else
+      cudaGetLastError();   // fall back to the SIMT form
+  }
+  int launches = 0;
+  const cudaError_t e = k_outer_source_groups(qi, slgg, mat, flux, q2, c->d_odm_tab, G,
+                                              c->cfg.nmat, c->cfg.nmom, c->M, c->C, g_lo, g_n,
+                                              &launches, st);
+  c->launches += launches;
+  return e;
+}
+
 int snap_create(const snap_config *cfg, int device, snap_ctx **out) {
   if (!cfg || !out) return fail(SNAP_ERR_BAD_ARG, "null argument");
   *out = nullptr;
@@ -726,6 +753,14 @@ int snap_create(const snap_config *cfg, int device, snap_ctx **out) {
     }
     c->grid_tc = std::min(blocks * sms, c->n_pair_items);
   }
+  // the outer source's fragment table, so that solves allocate nothing for it
+  {
+    const size_t words = outer_dmma_table_words(G, G, c->cfg.nmat, c->cfg.nmom);
+    if (cudaMalloc((void **)&c->d_odm_tab, sizeof(double) * words) == cudaSuccess)
+      c->odm_tab_words = words;
+    else
+      cudaGetLastError();
+  }
   *out = c;
   return SNAP_OK;
 }
@@ -765,16 +800,15 @@ int snap_expand_scattering_xs(snap_ctx *c, const double *slgg, const int32_t *ma
 int snap_calc_outer_source(snap_ctx *c, const double *qi, const double *slgg, const int32_t *mat,
                            const double *flux, double *q2grp, void *stream) {
   if (!c || !qi || !slgg || !mat || !flux || !q2grp) return fail(SNAP_ERR_BAD_ARG, "null argument");
-  SNAP_CUDA(k_outer_source(qi, slgg, mat, flux, q2grp, c->cfg.ng, c->cfg.nmat, c->cfg.nmom, c->M,
-                           c->C, (cudaStream_t)stream));
-  ++c->launches;
+  SNAP_CUDA(outer_source(c, qi, slgg, mat, flux, q2grp, c->cfg.ng, 0, c->cfg.ng,
+                         (cudaStream_t)stream));
   return SNAP_OK;
 }
 
 int snap_calc_outer_source_tc(snap_ctx *c, const double *qi, const double *slgg,
                               const int32_t *mat, const double *flux, double *q2grp, void *stream) {
   if (!c || !qi || !slgg || !mat || !flux || !q2grp) return fail(SNAP_ERR_BAD_ARG, "null argument");
-  if (outer_tc_smem_bytes(c->cfg.ng, c->cfg.nmat, c->cfg.nmom) > 200 * 1024 || c->cfg.nmat > 32)
+  if (!outer_tc_supported(c->cfg.ng, c->cfg.nmat, c->cfg.nmom))
     return fail(SNAP_ERR_UNSUPPORTED, "too many groups or materials for the tensor-core outer source");
   if (!c->d_scat_tc) {
     const size_t words = outer_tc_table_words(c->cfg.ng, c->cfg.nmat, c->cfg.nmom);
@@ -785,7 +819,8 @@ int snap_calc_outer_source_tc(snap_ctx *c, const double *qi, const double *slgg,
     }
   }
   SNAP_CUDA(k_outer_source_tc(qi, slgg, mat, flux, q2grp, c->d_scat_tc, c->cfg.ng, c->cfg.nmat,
-                              c->cfg.nmom, c->M, c->C, (cudaStream_t)stream));
+                              c->cfg.nmom, c->M, c->C, c->error(), c->timeout_ns,
+                              (cudaStream_t)stream));
   c->launches += 2;
   return SNAP_OK;
 }
@@ -796,9 +831,8 @@ int snap_calc_outer_source_groups(snap_ctx *c, int g_lo, int ng_total, const dou
   if (!c || !qi || !slgg || !mat || !flux_all || !q2grp) return fail(SNAP_ERR_BAD_ARG, "null argument");
   if (g_lo < 0 || ng_total < 1 || g_lo + c->cfg.ng > ng_total)
     return fail(SNAP_ERR_BAD_ARG, "group range outside the table");
-  SNAP_CUDA(k_outer_source_groups(qi, slgg, mat, flux_all, q2grp, ng_total, c->cfg.nmat,
-                                  c->cfg.nmom, c->M, c->C, g_lo, c->cfg.ng, (cudaStream_t)stream));
-  ++c->launches;
+  SNAP_CUDA(outer_source(c, qi, slgg, mat, flux_all, q2grp, ng_total, g_lo, c->cfg.ng,
+                         (cudaStream_t)stream));
   return SNAP_OK;
 }
 
@@ -1042,7 +1076,7 @@ int solve_impl(snap_ctx *c, const int32_t *mat, const double *qi, const double *
     // precision form: BF16 tensor-core outer source while far from convergence
     const bool lowp = c->fp32 && !(getenv("SNAP_B200_FP32_EXACT_OUTER") &&
                                    atoi(getenv("SNAP_B200_FP32_EXACT_OUTER")) != 0) &&
-                      outer_tc_smem_bytes(G, c->cfg.nmat, nmom) <= 200 * 1024 && c->cfg.nmat <= 32;
+                      outer_tc_supported(G, c->cfg.nmat, nmom);
     // outer change above which the low-precision source is used: ten times
     // the outer convergence tolerance, so the outer iterations that can
     // converge run on the FP64 source
@@ -1075,8 +1109,7 @@ int solve_impl(snap_ctx *c, const int32_t *mat, const double *qi, const double *
           if (rc) goto done;
           ++info->outers_lowp;
         } else {
-          STEP(k_outer_source(qi, slgg, mat, flux, q2grp, G, c->cfg.nmat, nmom, M, C, st));
-          ++c->launches;
+          STEP(outer_source(c, qi, slgg, mat, flux, q2grp, G, 0, G, st));
         }
         STEP(k_moment0(flux, fpo, M, n, st));                        // save_fluxes -> flux0po
         ++c->launches;
@@ -1469,9 +1502,9 @@ int snap_adjoint_solve(snap_ctx *c, const int32_t *mat, const double *qi, const 
     // the forward operator at the converged flux: total source
     ASTEP(k_expand_scat(slgg, mat, c->s_sxs, G, c->cfg.nmat, nmom, C, st));
     if (f32) ASTEP(k_to_f32(t_xs, (float *)c->s_txsw, n, st));
-    ASTEP(k_outer_source(qi, slgg, mat, flux, c->s_q2, G, c->cfg.nmat, nmom, M, C, st));
+    ASTEP(outer_source(c, qi, slgg, mat, flux, c->s_q2, G, 0, G, st));
     ASTEP(k_inner_source(c->s_sxs, c->s_q2, flux, qtot, f32, G, nmom, M, C, st));
-    c->launches += f32 ? 4 : 3;
+    c->launches += f32 ? 3 : 2;
     // forward sweep recording the cell-average fluxes and fixup flags (with
     // batches: recorded inside every adjoint application)
     if (batch >= G) {

@@ -75,7 +75,13 @@ def test_expand_cross_sections(d):
     assert np.array_equal(s_xs, os_)
 
 
-@pytest.mark.parametrize("d", [P.deck(1), P.Deck(16, 8, 8, nang=12, ng=5, nmom=4)])
+@pytest.mark.parametrize("d", [
+    P.deck(1), P.Deck(16, 8, 8, nang=12, ng=5, nmom=4),
+    P.Deck(16, 16, 8, nang=12, ng=32, nmom=4),    # deck-2 groups and moments (4 x 8 output tiles)
+    P.Deck(8, 8, 8, nang=12, ng=64, nmom=3),      # deck-3/5 groups and moments
+    P.Deck(7, 5, 3, nang=4, ng=9, nmom=2),        # ragged cell tile and group tiles
+    P.Deck(8, 4, 4, nang=4, ng=70, nmom=1),       # beyond 64 groups: the SIMT form
+], ids=lambda d: f"{d.nx}x{d.ny}x{d.nz}_G{d.ng}_M{d.cmom}")
 def test_outer_and_inner_source(d):
     prob = P.make_problem(d)
     o = Oracle(d)
@@ -364,16 +370,22 @@ def test_fp32_tf32_solve_error(tf32_sweep):
     assert rel_err(flux[..., 0].cpu().numpy(), ref[..., 0]) < FP32_TOL
 
 
-# --------------------------------- outer source on the BF16 tensor cores
+# --------------------------- outer source on the tcgen05 tensor cores (BF16)
 @pytest.mark.parametrize("d", [P.Deck(16, 16, 16, nang=4, ng=20, nmom=4),
                                P.Deck(16, 16, 8, nang=4, ng=4, nmom=1),
-                               P.Deck(16, 16, 8, nang=4, ng=33, nmom=3)],
-                         ids=["G20_cmom16", "G4_cmom1", "G33_cmom9"])
+                               P.Deck(16, 16, 8, nang=4, ng=33, nmom=3),
+                               P.Deck(16, 16, 8, nang=4, ng=32, nmom=4),
+                               P.Deck(16, 8, 8, nang=4, ng=64, nmom=3),
+                               P.Deck(7, 5, 3, nang=4, ng=32, nmom=4)],
+                         ids=["G20_cmom16", "G4_cmom1", "G33_cmom9", "G32_cmom16", "G64_cmom9",
+                              "ragged_cells"])
 def test_outer_source_tc_matches_fp64(d):
-    """The split-BF16 tensor-core outer source against the FP64 one (itself at
-    1e-12 of the oracle): the scattering term within 1e-4 of its largest
-    magnitude per moment, the fixed source exact, on tiles that mix the two
-    materials and group counts that are not multiples of 16."""
+    """The split-BF16 tensor-core outer source (tcgen05.mma, accumulators in
+    tensor memory) against the FP64 one (itself at 1e-12 of the oracle): the
+    scattering term within 1e-4 of its largest magnitude per moment, the
+    fixed source exact, on 128-cell tiles that mix the two materials, group
+    counts that are not multiples of 16 and a last tile that is mostly
+    empty."""
     snap = snap_ctx(d)
     dp = snap.device_problem(P.make_problem(d))
     flux = dev(random_qtot(d, 5))
