@@ -284,17 +284,19 @@ def gpu_inner_grind(d, steps, warmup, local, precision="fp64"):
 
 
 MIXED_PRECISION = ("fp32 sweep (moment contractions on FP64 tensor cores); group-to-group "
-                   "outer source on BF16 tensor cores (split operands, fp32 accumulation) while "
-                   "some scalar flux changes by more than 1000*epsi per outer, fp64 source for "
-                   "the final outers; fp64 octant sums, inner sources and convergence")
+                   "outer source on the tcgen05 tensor cores (split BF16 operands, fp32 "
+                   "accumulation in tensor memory) while some scalar flux changes by more than "
+                   "1000*epsi per outer, fp64 tensor-core source for the final outers; fp64 "
+                   "octant sums, inner sources and convergence")
 
 
 def outer_source_times(snap, snap32, dp, flux, reps=5):
-    """Device time of one outer source: FP64 kernel against the BF16
-    tensor-core kernel, on the same flux."""
+    """Device time of one outer source: the FP64 tensor-core (DMMA) kernel
+    against the split-BF16 tcgen05 kernel, on the same flux."""
     import torch
     out = {}
-    for name, fn in (("fp64_ms", snap.calc_outer_source), ("bf16_tc_ms", snap32.calc_outer_source_tc)):
+    for name, fn in (("fp64_dmma_ms", snap.calc_outer_source),
+                     ("bf16_tcgen05_ms", snap32.calc_outer_source_tc)):
         fn(dp["qi"], dp["slgg"], dp["mat"], flux)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -305,7 +307,7 @@ def outer_source_times(snap, snap32, dp, flux, reps=5):
         e1.record()
         torch.cuda.synchronize()
         out[name] = e0.elapsed_time(e1) / reps
-    out["speedup"] = out["fp64_ms"] / out["bf16_tc_ms"]
+    out["speedup"] = out["fp64_dmma_ms"] / out["bf16_tcgen05_ms"]
     return out
 
 

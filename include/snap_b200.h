@@ -93,19 +93,27 @@ int snap_expand_scattering_xs(snap_ctx *ctx, const double *slgg, const int32_t *
 /* q2grp[(g*C+c)*cmom + 0] = qi[g*C+c] + sum_{g'!=g} slgg[g][mat][g'][0] flux[g'][c][0]
  * q2grp[(g*C+c)*cmom + k] = sum_{g'!=g} slgg[g][mat][g'][l(k)] flux[g'][c][k]
  * Replaces CalcOuterSource (outer.cc:220-284 -> run_flux0_outer_source /
- * run_fluxm_outer_source, gpu_outer.cu:76-441).  Always double. */
+ * run_fluxm_outer_source, gpu_outer.cu:76-441).  Always double; the
+ * contraction runs on the FP64 tensor cores (mma.m8n8k4.f64) up to 64 groups
+ * per launch, so sums are taken in a different order than the reference's
+ * loop (rounding-level differences). */
 int snap_calc_outer_source(snap_ctx *ctx, const double *qi, const double *slgg,
                            const int32_t *mat, const double *flux, double *q2grp,
                            void *stream);
 
-/* The same outer source with the group-to-group contraction on the BF16
- * tensor cores: both operands split into two BF16 parts (three products,
+/* The same outer source with the group-to-group contraction on the
+ * fifth-generation tensor cores (tcgen05.mma kind::f16, accumulators in
+ * tensor memory): both operands split into two BF16 parts (three products,
  * FP32 accumulation), relative error of order 1e-5 of the scattering term;
  * qi is added in FP64.  Replaces CalcOuterSource (outer.cc:220-284) where a
  * low-precision source is acceptable: snap_transport_solve uses it in FP32
- * contexts only while the outer iteration is far from converged.
- * SNAP_ERR_UNSUPPORTED when the group count needs more shared memory than a
- * CTA has (about 300 groups). */
+ * contexts only while the outer iteration is far from converged, and only
+ * where its launch plan batches four moments (up to 32 groups with two
+ * materials, 64 with one).  Its waits are bounded: a timeout sets the
+ * device error word, which the next synchronising call reports.
+ * SNAP_ERR_UNSUPPORTED when the accumulators of one moment (groups rounded
+ * up to 16, times materials, twice) exceed the 512 tensor-memory columns or
+ * the operands the shared memory. */
 int snap_calc_outer_source_tc(snap_ctx *ctx, const double *qi, const double *slgg,
                               const int32_t *mat, const double *flux, double *q2grp,
                               void *stream);
@@ -201,7 +209,7 @@ typedef struct {
   int inners_per_outer[1024];
   double sweep_ms;     /* device time spent in the sweep kernels */
   double total_ms;     /* device time of the whole solve */
-  int outers_lowp;     /* outer iterations whose source came from the BF16 tensor cores */
+  int outers_lowp;     /* outer iterations whose source came from snap_calc_outer_source_tc */
   /* optional HOST array for the iteration log: records_cap entries, NULL
    * for none; records_len reports how many were written */
   snap_iter_record *records;

@@ -154,6 +154,9 @@ cudaError_t k_outer_source_groups(const double *qi, const double *slgg, const in
 // in *err after timeout_ns
 size_t outer_tc_table_words(int G, int nmat, int nmom);
 bool outer_tc_supported(int G, int nmat, int nmom);
+// whether the plan batches 4 moments (32-byte runs per input line); with
+// fewer the FP64 tensor-core form is the faster one
+bool outer_tc_preferred(int G, int nmat, int nmom);
 cudaError_t k_outer_source_tc(const double *qi, const double *slgg, const int32_t *mat,
                               const double *flux, double *q2grp, uint32_t *tab, int G, int nmat,
                               int nmom, int M, long long C, int *err, long long timeout_ns,

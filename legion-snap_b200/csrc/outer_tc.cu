@@ -171,7 +171,24 @@ __global__ void tcb_table_kernel(const double *__restrict__ slgg, int G, int nma
   }
 }
 
-__global__ void __launch_bounds__(TCR)
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// Warp roles: warps 0-3 convert the flux (thread = cell row of the tile),
+// warps 4-7 drain the accumulators (warp w owns tensor-memory lanes
+// 32(w-4)..32(w-4)+31), one thread of warp 8 issues the MMAs.  A batch is
+// (tile of 128 cells, MC consecutive moments); its operands and
+// accumulators are double-buffered (buffer = batch parity), with mbarriers
+//   full[buf]: the converted operands are in shared memory (128 arrivals),
+//   mma[buf]:  the batch's MMAs are done (tcgen05.commit): the operands may
+//              be overwritten and the accumulators read,
+//   free[buf]: the accumulators have been read (128 arrivals),
+// so the conversion of batch b+1 and the drain of batch b-1 overlap the
+// MMAs of batch b.
+constexpr int TC_THREADS = 9 * 32;
+
+__global__ void __launch_bounds__(TC_THREADS)
     outer_source_tc_kernel(const double *__restrict__ qi, const __nv_bfloat16 *__restrict__ tab,
                            const int32_t *__restrict__ mat, const double *__restrict__ flux,
                            double *__restrict__ q2grp, int G, int N, int KP, int nmat, int nmom,
@@ -179,18 +196,25 @@ __global__ void __launch_bounds__(TCR)
                            long long timeout_ns) {
   extern __shared__ __align__(1024) unsigned char tc_smem[];
   const size_t b_tile = (size_t)N * KP * 2, a_tile = (size_t)TCR * KP * 2;
-  const size_t b_bytes = (size_t)nmom * nmat * 2 * b_tile;
-  unsigned char *sB = tc_smem;                 // [l][mat][hi, lo] N x KP
-  unsigned char *sA = tc_smem + b_bytes;       // [moment of the batch][hi, lo] 128 x KP
-  __shared__ __align__(8) uint64_t s_bar[2];   // 0: table copy, 1: MMA completion
+  const size_t b_bytes = (size_t)nmom * nmat * 2 * b_tile, a_buf = (size_t)MC * 2 * a_tile;
+  unsigned char *sB = tc_smem;            // [l][mat][hi, lo] N x KP
+  unsigned char *sA = tc_smem + b_bytes;  // [buf][moment of the batch][hi, lo] 128 x KP
+  __shared__ __align__(8) uint64_t s_bar[7];   // tab, full[2], mma[2], free[2]
   __shared__ uint32_t s_tmem;
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const uint32_t bar_tab = smem_u32(&s_bar[0]), bar_mma = smem_u32(&s_bar[1]);
-  const uint32_t idesc = idesc_bf16(N);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t bar_tab = smem_u32(&s_bar[0]);
+  auto bar_full = [&](int b) { return smem_u32(&s_bar[1 + b]); };
+  auto bar_mma = [&](int b) { return smem_u32(&s_bar[3 + b]); };
+  auto bar_free = [&](int b) { return smem_u32(&s_bar[5 + b]); };
+  const int tcols = MC * nmat * N;   // accumulator columns of one buffer
 
   if (tid == 0) {
     mbar_init(bar_tab, 1);
-    mbar_init(bar_mma, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(bar_full(b), TCR);
+      mbar_init(bar_mma(b), 1);
+      mbar_init(bar_free(b), TCR);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
@@ -204,35 +228,24 @@ __global__ void __launch_bounds__(TCR)
   __syncthreads();
   fence_after_sync();
   const uint32_t tmem = s_tmem;
-  // the scattering operands of every band and material: bulk copies
-  if (tid == 0) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_tab),
-                 "r"((uint32_t)b_bytes)
-                 : "memory");
-    for (size_t off = 0; off < b_bytes; off += 16384) {
-      const uint32_t len = (uint32_t)(b_bytes - off < 16384 ? b_bytes - off : 16384);
-      asm volatile(
-          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-              smem_u32(sB + off)),
-          "l"((const unsigned char *)tab + off), "r"(len), "r"(bar_tab)
-          : "memory");
-    }
-  }
-  // (every wait's outcome is made CTA-uniform before anyone acts on it, so
-  // that all threads meet the same barriers)
-  bool ok = __syncthreads_and(tid != 0 || mbar_wait(bar_tab, 0, err, timeout_ns));
 
-  uint32_t commits = 0;
+  const int nbt = (M + MC - 1) / MC;   // batches per tile
   const long long ntiles = (C + TCR - 1) / TCR;
+  const long long my_tiles = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const long long nb = my_tiles * nbt;
+  auto batch_tile = [&](long long b) { return blockIdx.x + (b / nbt) * (long long)gridDim.x; };
   const bool runs4 = (M & 3) == 0;   // a batch of 4 moments is one aligned 32-byte run
-  for (long long tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x) {
-    const long long c = tile * TCR + tid;   // this thread's cell = A row = accumulator lane
-    const bool valid = c < C;
-    const int matr = valid ? mat[c] - 1 : -1;
-    for (int m0 = 0; ok && m0 < M; m0 += MC) {
-      const int mc = min(MC, M - m0);
-      // the batch's split flux: each (input group, cell) run of mc moments is
-      // read once and converted into row tid of the batch's A operands
+
+  if (warp < 4) {
+    // ---- conversion: cell row tid of each batch's operands
+    for (long long b = 0; b < nb; ++b) {
+      const int buf = (int)(b & 1);
+      const uint32_t use = (uint32_t)(b >> 1);
+      if (use > 0 && !mbar_wait(bar_mma(buf), (use - 1) & 1u, err, timeout_ns)) break;
+      const long long c = batch_tile(b) * TCR + tid;
+      const bool valid = c < C;
+      const int m0 = (int)(b % nbt) * MC, mc = min(MC, M - m0);
+      unsigned char *A = sA + (size_t)buf * a_buf;
       for (int k8 = 0; k8 < KP; k8 += 8) {
         double x[8][MCMAX];
 #pragma unroll
@@ -258,43 +271,29 @@ __global__ void __launch_bounds__(TCR)
           __align__(16) __nv_bfloat16 h[8], lo[8];
 #pragma unroll
           for (int e = 0; e < 8; ++e) split_bf16(x[e][mm], h[e], lo[e]);
-          unsigned char *t = sA + (size_t)mm * 2 * a_tile;
+          unsigned char *t = A + (size_t)mm * 2 * a_tile;
           *(uint4 *)(t + off) = *(const uint4 *)h;
           *(uint4 *)(t + a_tile + off) = *(const uint4 *)lo;
         }
       }
-      // make the operands visible to the tensor cores, then one thread issues:
-      // moment mm, material mi -> accumulator columns (mm * nmat + mi) * N
+      // visible to the tensor cores, then count this row in
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      __syncthreads();
-      if (tid == 0) {
-        fence_after_sync();
-        for (int mm = 0; mm < mc; ++mm) {
-          const int k = m0 + mm;
-          int l = 0;
-          while ((l + 1) * (l + 1) <= k) ++l;
-          const uint32_t a_hi = smem_u32(sA + (size_t)mm * 2 * a_tile), a_lo = a_hi + (uint32_t)a_tile;
-          for (int mi = 0; mi < nmat; ++mi) {
-            const uint32_t d = tmem + (uint32_t)((mm * nmat + mi) * N);
-            const uint32_t b_hi = smem_u32(sB + ((size_t)l * nmat + mi) * 2 * b_tile),
-                           b_lo = b_hi + (uint32_t)b_tile;
-            for (int s = 0; s < KP / 16; ++s) {
-              const uint32_t ao = (uint32_t)s * (TCR / 8) * 256, bo = (uint32_t)s * (N / 8) * 256;
-              mma_bf16(d, smem_desc(a_hi + ao), smem_desc(b_hi + bo), idesc, s > 0);
-              mma_bf16(d, smem_desc(a_hi + ao), smem_desc(b_lo + bo), idesc, 1);
-              mma_bf16(d, smem_desc(a_lo + ao), smem_desc(b_hi + bo), idesc, 1);
-            }
-          }
-        }
-        mma_commit(bar_mma);
-      }
-      ++commits;
-      // accumulators of the batch: wait, read this thread's lane (its cell's
-      // material), store
-      ok = __syncthreads_and(mbar_wait(bar_mma, (commits - 1) & 1u, err, timeout_ns));
-      if (!ok) break;
+      mbar_arrive(bar_full(buf));
+    }
+  } else if (warp < 8) {
+    // ---- drain: lane row 32(warp-4) + lane of each batch's accumulators
+    const int row = (warp - 4) * 32 + lane;
+    const uint32_t lane_addr = tmem + ((uint32_t)((warp - 4) * 32) << 16);
+    for (long long b = 0; b < nb; ++b) {
+      const int buf = (int)(b & 1);
+      const uint32_t use = (uint32_t)(b >> 1);
+      if (!mbar_wait(bar_mma(buf), use & 1u, err, timeout_ns)) break;
       fence_after_sync();
-      const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+      const long long c = batch_tile(b) * TCR + row;
+      const bool valid = c < C;
+      const int matr = valid ? mat[c] - 1 : -1;
+      const int m0 = (int)(b % nbt) * MC, mc = min(MC, M - m0);
+      const uint32_t tb = lane_addr + (uint32_t)(buf * tcols);
       for (int gb = 0; gb < N; gb += 16) {
         float v[MCMAX][16];
 #pragma unroll
@@ -302,7 +301,7 @@ __global__ void __launch_bounds__(TCR)
           if (mm >= mc) break;
           for (int mi = 0; mi < nmat; ++mi) {
             float t[16];
-            tmem_ld16(lane_addr + (uint32_t)((mm * nmat + mi) * N + gb), t);
+            tmem_ld16(tb + (uint32_t)((mm * nmat + mi) * N + gb), t);
             tmem_wait_ld();
             if (mi == matr) {
 #pragma unroll
@@ -330,11 +329,55 @@ __global__ void __launch_bounds__(TCR)
           }
         }
       }
-      // the next batch overwrites the A operands and the accumulators
       fence_before_sync();
-      __syncthreads();
+      mbar_arrive(bar_free(buf));
+    }
+  } else if (lane == 0) {
+    // ---- MMA issue: moment mm, material mi -> columns buf * tcols + (mm * nmat + mi) * N
+    const uint32_t idesc = idesc_bf16(N);
+    if (nb > 0) {
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_tab),
+                   "r"((uint32_t)b_bytes)
+                   : "memory");
+      for (size_t off = 0; off < b_bytes; off += 16384) {
+        const uint32_t len = (uint32_t)(b_bytes - off < 16384 ? b_bytes - off : 16384);
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                smem_u32(sB + off)),
+            "l"((const unsigned char *)tab + off), "r"(len), "r"(bar_tab)
+            : "memory");
+      }
+    }
+    bool ok = nb == 0 || mbar_wait(bar_tab, 0, err, timeout_ns);
+    for (long long b = 0; ok && b < nb; ++b) {
+      const int buf = (int)(b & 1);
+      const uint32_t use = (uint32_t)(b >> 1);
+      if (!mbar_wait(bar_full(buf), use & 1u, err, timeout_ns)) break;
+      if (use > 0 && !mbar_wait(bar_free(buf), (use - 1) & 1u, err, timeout_ns)) break;
+      fence_after_sync();
+      const int m0 = (int)(b % nbt) * MC, mc = min(MC, M - m0);
+      const unsigned char *A = sA + (size_t)buf * a_buf;
+      for (int mm = 0; mm < mc; ++mm) {
+        const int k = m0 + mm;
+        int l = 0;
+        while ((l + 1) * (l + 1) <= k) ++l;
+        const uint32_t a_hi = smem_u32(A + (size_t)mm * 2 * a_tile), a_lo = a_hi + (uint32_t)a_tile;
+        for (int mi = 0; mi < nmat; ++mi) {
+          const uint32_t d = tmem + (uint32_t)(buf * tcols + (mm * nmat + mi) * N);
+          const uint32_t b_hi = smem_u32(sB + ((size_t)l * nmat + mi) * 2 * b_tile),
+                         b_lo = b_hi + (uint32_t)b_tile;
+          for (int s = 0; s < KP / 16; ++s) {
+            const uint32_t ao = (uint32_t)s * (TCR / 8) * 256, bo = (uint32_t)s * (N / 8) * 256;
+            mma_bf16(d, smem_desc(a_hi + ao), smem_desc(b_hi + bo), idesc, s > 0);
+            mma_bf16(d, smem_desc(a_hi + ao), smem_desc(b_lo + bo), idesc, 1);
+            mma_bf16(d, smem_desc(a_lo + ao), smem_desc(b_hi + bo), idesc, 1);
+          }
+        }
+      }
+      mma_commit(bar_mma(buf));
     }
   }
+  // every role has finished (or given up); the drain waited for the last MMAs
   fence_before_sync();
   __syncthreads();
   if (warp == 0) {
@@ -358,12 +401,12 @@ bool tc_plan(int G, int nmat, int nmom, TcPlan *pl) {
   pl->KP = pad16(G);
   const size_t b_bytes = (size_t)nmom * nmat * 2 * pl->N * pl->KP * 2;
   for (int mc = MCMAX; mc >= 1; mc /= 2) {
-    const size_t smem = b_bytes + (size_t)mc * 2 * TCR * pl->KP * 2;
-    if ((long long)mc * nmat * pl->N <= 512 && smem <= 200 * 1024) {
+    const size_t smem = b_bytes + 2 * (size_t)mc * 2 * TCR * pl->KP * 2;   // two operand buffers
+    if (2LL * mc * nmat * pl->N <= 512 && smem <= 220 * 1024) {            // two accumulator buffers
       pl->MC = mc;
       pl->smem = smem;
       pl->cols = 32;
-      while (pl->cols < mc * nmat * pl->N) pl->cols <<= 1;
+      while (pl->cols < 2 * mc * nmat * pl->N) pl->cols <<= 1;
       return true;
     }
   }
@@ -380,6 +423,11 @@ size_t outer_tc_table_words(int G, int nmat, int nmom) {
 bool outer_tc_supported(int G, int nmat, int nmom) {
   TcPlan pl;
   return tc_plan(G, nmat, nmom, &pl);
+}
+
+bool outer_tc_preferred(int G, int nmat, int nmom) {
+  TcPlan pl;
+  return tc_plan(G, nmat, nmom, &pl) && pl.MC == MCMAX;
 }
 
 cudaError_t k_outer_source_tc(const double *qi, const double *slgg, const int32_t *mat,
@@ -408,11 +456,11 @@ cudaError_t k_outer_source_tc(const double *qi, const double *slgg, const int32_
   // resident CTAs: by shared memory (with the static part and the per-CTA
   // reserve), by the 512 tensor-memory columns, by registers
   const int by_smem = (int)((size_t)smem_sm / (pl.smem + 2048));
-  const int by_regs = 65536 / (((fa.numRegs + 7) / 8 * 8) * TCR);
+  const int by_regs = 65536 / (((fa.numRegs + 7) / 8 * 8) * TC_THREADS);
   const int blocks = std::max(1, std::min(std::min(by_smem, 512 / pl.cols), by_regs));
   const long long tiles = (C + TCR - 1) / TCR;
   const int grid = (int)std::min<long long>(tiles, (long long)blocks * sms);
-  outer_source_tc_kernel<<<grid, TCR, pl.smem, st>>>(qi, (const __nv_bfloat16 *)tab, mat, flux,
+  outer_source_tc_kernel<<<grid, TC_THREADS, pl.smem, st>>>(qi, (const __nv_bfloat16 *)tab, mat, flux,
                                                      q2grp, G, pl.N, pl.KP, nmat, nmom, M, pl.MC,
                                                      C, pl.cols, err, timeout_ns);
   return cudaGetLastError();

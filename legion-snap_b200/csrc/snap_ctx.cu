@@ -1073,10 +1073,12 @@ int solve_impl(snap_ctx *c, const int32_t *mat, const double *qi, const double *
       ++c->launches;
     }
     STEP(cudaMemsetAsync(flux, 0, sizeof(double) * n * M, st));   // snap.cc:313-316
-    // precision form: BF16 tensor-core outer source while far from convergence
+    // precision form: split-BF16 tcgen05 outer source while far from
+    // convergence, where its plan batches 4 moments (else the FP64
+    // tensor-core source is the faster one)
     const bool lowp = c->fp32 && !(getenv("SNAP_B200_FP32_EXACT_OUTER") &&
                                    atoi(getenv("SNAP_B200_FP32_EXACT_OUTER")) != 0) &&
-                      outer_tc_supported(G, c->cfg.nmat, nmom);
+                      outer_tc_preferred(G, c->cfg.nmat, nmom);
     // outer change above which the low-precision source is used: ten times
     // the outer convergence tolerance, so the outer iterations that can
     // converge run on the FP64 source

@@ -104,8 +104,9 @@ class Snap:
         return q2
 
     def calc_outer_source_tc(self, qi, slgg, mat, flux) -> torch.Tensor:
-        """The outer source with the group-to-group contraction on the BF16
-        tensor cores (split operands, FP32 accumulation)."""
+        """The outer source with the group-to-group contraction on the
+        tcgen05 tensor cores (split BF16 operands, FP32 accumulation in tensor
+        memory)."""
         q2 = self._empty(self.deck.ng, self.C, self.deck.cmom)
         abi.check(self.lib.snap_calc_outer_source_tc(self.handle, _ptr(qi), _ptr(slgg), _ptr(mat),
                                                      _ptr(flux), _ptr(q2), _stream()))
