@@ -5,19 +5,17 @@
 // Same result as the FP64 outer source (kernels.cu; reference:
 // CalcOuterSource, outer.cc:107-217, gpu_outer.cu:76-441):
 //   q2[g][c][k] = qi[g][c] [k = 0] + sum_{g' != g} slgg[g][mat(c)][g'][l(k)] phi[g'][c][k]
-// For one moment k (hence band l) and 128 cells this is a GEMM
-//   D[c][g] = sum_{g'} A[c][g'] B[g][g'],   A = phi[.][c][k], B = S_l,mat
-// with the cells as the MMA's M = 128 rows (tensor-memory lanes), the output
-// groups as N and the input groups as K.  BF16 keeps 8 mantissa bits, so
-// both operands are split x = hi + lo (hi the BF16 rounding of x, lo that of
-// the remainder) and the product is accumulated as hi*hi + hi*lo + lo*hi:
-// relative error of order 2^-16.  That is not the FP64 source: the solve
-// driver uses this only while the outer iteration is still far from
-// converged and switches to the FP64 source for the final outer iterations
-// (a mixed-precision refinement: the converged fixed point is the one of the
-// FP64 source).  Cells of different materials: the A operand is staged once
-// per material with the rows of other materials zeroed, and the materials'
-// products accumulate into the same tensor-memory tile.
+// For 128 (cell, moment) rows this is a GEMM per band l and material
+//   D[(c,k)][g] = sum_{g'} A[(c,k)][g'] B[g][g'],   A = phi[g'][c][k], B = S_l,mat
+// with the rows as the MMA's M = 128 (tensor-memory lanes), the output
+// groups as N and the input groups as K; each row keeps the result of its
+// own band and material.  BF16 keeps 8 mantissa bits, so both operands are
+// split x = hi + lo (hi the BF16 rounding of x, lo that of the remainder)
+// and the product is accumulated as hi*hi + hi*lo + lo*hi: relative error
+// of order 2^-16.  That is not the FP64 source: the solve driver uses this
+// only while the outer iteration is still far from converged and switches to
+// the FP64 source for the final outer iterations (a mixed-precision
+// refinement: the converged fixed point is the one of the FP64 source).
 //
 // Operands live in shared memory in the K-major layout without swizzle:
 // 8-row x 16-byte core matrices, the two core matrices of one 16-element K
@@ -25,13 +23,12 @@
 // bytes apart (stride byte offset), K steps one after another.  The
 // scattering operands of every band and material (built per call by
 // tcb_table_kernel in that layout) are copied into shared memory once per
-// CTA with one bulk copy (cp.async.bulk, completion on an mbarrier).  Per
-// moment the 128 threads convert their cell's flux to the split operands,
-// one elected thread issues the MMAs and commits them to an mbarrier, and
-// every MC moments the four warps read their 32 lanes of the accumulators
-// back (tcgen05.ld) and store the MC consecutive moments of each (group,
-// cell) as one 32-byte run.  Every wait is bounded and records a timeout in
-// the device error word.
+// CTA with bulk copies (cp.async.bulk, completion on an mbarrier).  The
+// MMA rows are (cell, moment) pairs of whole cells, so the flux is read and
+// the source written in whole per-cell lines of moments; conversion, MMA
+// issue and the drain of the accumulators (tcgen05.ld) run in separate warps
+// on double-buffered operands (see the kernel).  Every wait is bounded and
+// records a timeout in the device error word.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -44,7 +41,6 @@ namespace snapb200 {
 namespace {
 
 constexpr int TCR = 128;   // cells per tile = MMA rows; 4 warps, warp w owns lanes 32w..32w+31
-constexpr int MCMAX = 4;   // moments per accumulator batch
 
 __host__ __device__ inline int pad16(int x) { return (x + 15) / 16 * 16; }
 
@@ -73,6 +69,10 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p) {
 
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
 // Waits until the phase with parity `parity` of the mbarrier has completed.
@@ -171,42 +171,60 @@ __global__ void tcb_table_kernel(const double *__restrict__ slgg, int G, int nma
   }
 }
 
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
+// A batch is CPB = floor(128 / cmom) cells with all their moments: MMA row
+// r = (cell r / cmom, moment r % cmom).  For one input group the batch's flux
+// is one contiguous run of CPB * cmom doubles, so a loader thread streams it
+// into a shared-memory stage with one bulk copy per input group (S stages in
+// flight); the converting threads read it from there.  Rows of different
+// bands and materials need different B operands: each row is staged once per
+// material with the rows of other materials zeroed, the batch's MMAs run
+// once per (band, material) and accumulate the materials into one tile per
+// band (nmom tiles of N columns), and each row keeps the tile of its own
+// band, so the source is written in whole per-cell lines of moments too.
+// Warp roles: warps 0-3 convert (thread = row), warps 4-7 drain the
+// accumulators (warp w owns tensor-memory lanes 32(w-4)..32(w-4)+31), lane 0
+// of warp 8 issues the MMAs, lane 0 of warp 9 loads.  Operands are
+// double-buffered when two sets fit the shared memory (NA = 2; buffer =
+// batch % NA), accumulators when two sets fit the 512 tensor-memory columns
+// (TB = 2), with mbarriers
+//   raw[st] / rawfree[st]: a stage holds a batch's flux / has been converted,
+//   full[buf]:  the converted operands are in shared memory (128 arrivals),
+//   mma[buf]:   the batch's MMAs are done (tcgen05.commit): the operands may
+//               be overwritten and the accumulators read,
+//   free[tbuf]: the accumulators have been read (128 arrivals),
+// so loads run S batches ahead and the conversion of batch b+1 and the
+// drain of batch b-1 overlap the MMAs of batch b.  S = 0 (no room for a
+// stage, or runs not 16-byte aligned): the converting threads load the flux
+// themselves.
+constexpr int TC_THREADS = 10 * 32;
+constexpr int TC_MAX_STAGES = 4;
 
-// Warp roles: warps 0-3 convert the flux (thread = cell row of the tile),
-// warps 4-7 drain the accumulators (warp w owns tensor-memory lanes
-// 32(w-4)..32(w-4)+31), one thread of warp 8 issues the MMAs.  A batch is
-// (tile of 128 cells, MC consecutive moments); its operands and
-// accumulators are double-buffered (buffer = batch parity), with mbarriers
-//   full[buf]: the converted operands are in shared memory (128 arrivals),
-//   mma[buf]:  the batch's MMAs are done (tcgen05.commit): the operands may
-//              be overwritten and the accumulators read,
-//   free[buf]: the accumulators have been read (128 arrivals),
-// so the conversion of batch b+1 and the drain of batch b-1 overlap the
-// MMAs of batch b.
-constexpr int TC_THREADS = 9 * 32;
-
-__global__ void __launch_bounds__(TC_THREADS)
+__global__ void __launch_bounds__(TC_THREADS, 1)
     outer_source_tc_kernel(const double *__restrict__ qi, const __nv_bfloat16 *__restrict__ tab,
                            const int32_t *__restrict__ mat, const double *__restrict__ flux,
                            double *__restrict__ q2grp, int G, int N, int KP, int nmat, int nmom,
-                           int M, int MC, long long C, int tmem_cols, int *err,
+                           int M, int NA, int TB, int S, long long C, int tmem_cols, int *err,
                            long long timeout_ns) {
   extern __shared__ __align__(1024) unsigned char tc_smem[];
+  const int CPB = TCR / M;   // cells per batch
   const size_t b_tile = (size_t)N * KP * 2, a_tile = (size_t)TCR * KP * 2;
-  const size_t b_bytes = (size_t)nmom * nmat * 2 * b_tile, a_buf = (size_t)MC * 2 * a_tile;
-  unsigned char *sB = tc_smem;            // [l][mat][hi, lo] N x KP
-  unsigned char *sA = tc_smem + b_bytes;  // [buf][moment of the batch][hi, lo] 128 x KP
-  __shared__ __align__(8) uint64_t s_bar[7];   // tab, full[2], mma[2], free[2]
+  const size_t b_bytes = (size_t)nmom * nmat * 2 * b_tile;
+  const size_t run = (size_t)CPB * M * sizeof(double), stage = run * G;
+  unsigned char *sB = tc_smem;                       // [l][mat][hi, lo] N x KP
+  unsigned char *sA = tc_smem + b_bytes;             // [buf][mat][hi, lo] 128 x KP
+  const size_t a_buf = (size_t)nmat * 2 * a_tile;
+  double *sQ = (double *)(sA + NA * a_buf);           // [2][cell][g]: qi of a batch (drain)
+  const double *sR = sQ + (size_t)2 * CPB * G;        // [stage][g'][CPB * M]
+  __shared__ __align__(8) uint64_t s_bar[7 + 2 * TC_MAX_STAGES];
   __shared__ uint32_t s_tmem;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t bar_tab = smem_u32(&s_bar[0]);
   auto bar_full = [&](int b) { return smem_u32(&s_bar[1 + b]); };
   auto bar_mma = [&](int b) { return smem_u32(&s_bar[3 + b]); };
   auto bar_free = [&](int b) { return smem_u32(&s_bar[5 + b]); };
-  const int tcols = MC * nmat * N;   // accumulator columns of one buffer
+  auto bar_raw = [&](int st) { return smem_u32(&s_bar[7 + st]); };
+  auto bar_rawfree = [&](int st) { return smem_u32(&s_bar[7 + TC_MAX_STAGES + st]); };
+  const int tcols = nmom * N;   // accumulator columns of one batch: a tile per band
 
   if (tid == 0) {
     mbar_init(bar_tab, 1);
@@ -214,6 +232,10 @@ __global__ void __launch_bounds__(TC_THREADS)
       mbar_init(bar_full(b), TCR);
       mbar_init(bar_mma(b), 1);
       mbar_init(bar_free(b), TCR);
+    }
+    for (int st = 0; st < S; ++st) {
+      mbar_init(bar_raw(st), 1);
+      mbar_init(bar_rawfree(st), TCR);
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -229,111 +251,127 @@ __global__ void __launch_bounds__(TC_THREADS)
   fence_after_sync();
   const uint32_t tmem = s_tmem;
 
-  const int nbt = (M + MC - 1) / MC;   // batches per tile
-  const long long ntiles = (C + TCR - 1) / TCR;
-  const long long my_tiles = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
-  const long long nb = my_tiles * nbt;
-  auto batch_tile = [&](long long b) { return blockIdx.x + (b / nbt) * (long long)gridDim.x; };
-  const bool runs4 = (M & 3) == 0;   // a batch of 4 moments is one aligned 32-byte run
+  const long long nbatches = (C + CPB - 1) / CPB;
+  const long long nb = blockIdx.x < nbatches ? (nbatches - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  auto batch_cell0 = [&](long long b) { return (blockIdx.x + b * (long long)gridDim.x) * CPB; };
+  // a batch is staged when it has all its cells (the last may not)
+  auto staged = [&](long long b) { return S > 0 && batch_cell0(b) + CPB <= C; };
 
-  if (warp < 4) {
-    // ---- conversion: cell row tid of each batch's operands
-    for (long long b = 0; b < nb; ++b) {
-      const int buf = (int)(b & 1);
-      const uint32_t use = (uint32_t)(b >> 1);
-      if (use > 0 && !mbar_wait(bar_mma(buf), (use - 1) & 1u, err, timeout_ns)) break;
-      const long long c = batch_tile(b) * TCR + tid;
-      const bool valid = c < C;
-      const int m0 = (int)(b % nbt) * MC, mc = min(MC, M - m0);
-      unsigned char *A = sA + (size_t)buf * a_buf;
-      for (int k8 = 0; k8 < KP; k8 += 8) {
-        double x[8][MCMAX];
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
-          const int gi = k8 + e;
-          const double *src = flux + ((size_t)gi * C + c) * M + m0;
-          if (valid && gi < G && mc == 4 && runs4) {
-            const double2 v0 = __ldg((const double2 *)src), v1 = __ldg((const double2 *)src + 1);
-            x[e][0] = v0.x;
-            x[e][1] = v0.y;
-            x[e][2] = v1.x;
-            x[e][3] = v1.y;
-          } else {
-#pragma unroll
-            for (int mm = 0; mm < MCMAX; ++mm)
-              x[e][mm] = (valid && gi < G && mm < mc) ? __ldg(src + mm) : 0.0;
-          }
+  if (warp < 8) {
+    // rows: thread tid (conversion) or lane row 32(warp-4) + lane (drain)
+    const int row = warp < 4 ? tid : (warp - 4) * 32 + lane;
+    const int rc = row / M, rm = row - rc * M;   // cell of the batch, moment
+    int rl = 0;
+    while ((rl + 1) * (rl + 1) <= rm) ++rl;      // band of the moment
+    if (warp < 4) {
+      // ---- conversion: row of each batch's operands (material of the
+      // next batch's cell loaded a batch ahead)
+      int mat_next = (nb > 0 && rc < CPB && batch_cell0(0) + rc < C) ? mat[batch_cell0(0) + rc] - 1 : -1;
+      for (long long b = 0; b < nb; ++b) {
+        const int buf = (int)(b % NA);
+        const uint32_t use = (uint32_t)(b / NA);
+        const int matr = mat_next;
+        {
+          const long long cn = batch_cell0(b + 1) + rc;
+          mat_next = (b + 1 < nb && rc < CPB && cn < C) ? mat[cn] - 1 : -1;
         }
-        const uint32_t off = kmajor_offset(TCR, tid, k8);
+        if (use > 0 && !mbar_wait(bar_mma(buf), (use - 1) & 1u, err, timeout_ns)) break;
+        const long long c = batch_cell0(b) + rc;
+        const bool valid = rc < CPB && c < C;
+        const bool from_stage = staged(b);
+        const int st = S > 0 ? (int)(b % S) : 0;
+        if (from_stage && !mbar_wait(bar_raw(st), (uint32_t)(b / S) & 1u, err, timeout_ns)) break;
+        const double *src = from_stage ? sR + (size_t)st * (stage / sizeof(double)) + row
+                                       : flux + ((size_t)(valid ? c : 0)) * M + rm;
+        const size_t gstride = from_stage ? (size_t)CPB * M : (size_t)C * M;
+        unsigned char *A = sA + (size_t)buf * a_buf;
+        for (int k8 = 0; k8 < KP; k8 += 8) {
+          double x[8];
 #pragma unroll
-        for (int mm = 0; mm < MCMAX; ++mm) {
-          if (mm >= mc) break;
+          for (int e = 0; e < 8; ++e) {
+            const int gi = k8 + e;
+            x[e] = (valid && gi < G) ? (from_stage ? src[gi * gstride] : __ldg(src + gi * gstride))
+                                     : 0.0;
+          }
           __align__(16) __nv_bfloat16 h[8], lo[8];
 #pragma unroll
-          for (int e = 0; e < 8; ++e) split_bf16(x[e][mm], h[e], lo[e]);
-          unsigned char *t = A + (size_t)mm * 2 * a_tile;
-          *(uint4 *)(t + off) = *(const uint4 *)h;
-          *(uint4 *)(t + a_tile + off) = *(const uint4 *)lo;
-        }
-      }
-      // visible to the tensor cores, then count this row in
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      mbar_arrive(bar_full(buf));
-    }
-  } else if (warp < 8) {
-    // ---- drain: lane row 32(warp-4) + lane of each batch's accumulators
-    const int row = (warp - 4) * 32 + lane;
-    const uint32_t lane_addr = tmem + ((uint32_t)((warp - 4) * 32) << 16);
-    for (long long b = 0; b < nb; ++b) {
-      const int buf = (int)(b & 1);
-      const uint32_t use = (uint32_t)(b >> 1);
-      if (!mbar_wait(bar_mma(buf), use & 1u, err, timeout_ns)) break;
-      fence_after_sync();
-      const long long c = batch_tile(b) * TCR + row;
-      const bool valid = c < C;
-      const int matr = valid ? mat[c] - 1 : -1;
-      const int m0 = (int)(b % nbt) * MC, mc = min(MC, M - m0);
-      const uint32_t tb = lane_addr + (uint32_t)(buf * tcols);
-      for (int gb = 0; gb < N; gb += 16) {
-        float v[MCMAX][16];
-#pragma unroll
-        for (int mm = 0; mm < MCMAX; ++mm) {
-          if (mm >= mc) break;
+          for (int e = 0; e < 8; ++e) split_bf16(x[e], h[e], lo[e]);
+          const uint32_t off = kmajor_offset(TCR, row, k8);
+          const uint4 zv = make_uint4(0, 0, 0, 0);
           for (int mi = 0; mi < nmat; ++mi) {
-            float t[16];
-            tmem_ld16(tb + (uint32_t)((mm * nmat + mi) * N + gb), t);
-            tmem_wait_ld();
-            if (mi == matr) {
-#pragma unroll
-              for (int j = 0; j < 16; ++j) v[mm][j] = t[j];
+            unsigned char *t = A + (size_t)mi * 2 * a_tile;
+            *(uint4 *)(t + off) = mi == matr ? *(const uint4 *)h : zv;
+            *(uint4 *)(t + a_tile + off) = mi == matr ? *(const uint4 *)lo : zv;
+          }
+        }
+        if (S > 0) mbar_arrive(bar_rawfree(st));   // the stage may be refilled
+        // visible to the tensor cores, then count this row in
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_arrive(bar_full(buf));
+      }
+    } else {
+      // ---- drain: this lane's row keeps the tile of its band.  The
+      // moment-0 row of each cell copies the cell's fixed source of the next
+      // batch into shared memory (cp.async) while this batch is drained.
+      const uint32_t lane_addr = tmem + ((uint32_t)((warp - 4) * 32) << 16);
+      const bool owns_q = rm == 0 && rc < CPB;
+      auto fetch_q = [&](long long b) {
+        if (owns_q && b < nb) {
+          const long long cq = batch_cell0(b) + rc;
+          double *q = sQ + ((size_t)(b & 1) * CPB + rc) * G;
+          for (int g = 0; g < G; ++g) {
+            if (cq < C) {
+              const unsigned sq = (unsigned)__cvta_generic_to_shared(q + g);
+              asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sq),
+                           "l"(qi + (size_t)g * C + cq)
+                           : "memory");
+            } else {
+              q[g] = 0.0;
             }
           }
         }
-        if (!valid) continue;
+        asm volatile("cp.async.commit_group;" ::: "memory");
+      };
+      fetch_q(0);
+      for (long long b = 0; b < nb; ++b) {
+        const int buf = (int)(b % NA), tbuf = (int)(b % TB);
+        if (!mbar_wait(bar_mma(buf), (uint32_t)(b / NA) & 1u, err, timeout_ns)) break;
+        fence_after_sync();
+        const long long c = batch_cell0(b) + rc;
+        const bool valid = rc < CPB && c < C;
+        const uint32_t tb = lane_addr + (uint32_t)(tbuf * tcols);
+        fetch_q(b + 1);
+        asm volatile("cp.async.wait_group 1;" ::: "memory");   // this batch's copies are in
+        for (int gb = 0; gb < N; gb += 16) {
+          // the fixed source of the block's groups (moment-0 rows)
+          const double *q = sQ + ((size_t)(b & 1) * CPB + (rc < CPB ? rc : 0)) * G;
+          double qv[16];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int g = gb + j;
-          if (g >= G) break;
-          double o[MCMAX];
+          for (int j = 0; j < 16; ++j) qv[j] = (valid && rm == 0 && gb + j < G) ? q[gb + j] : 0.0;
+          // every band's tile (at most 4), one wait, keep the row's band
+          float u[4][16], v[16];
 #pragma unroll
-          for (int mm = 0; mm < MCMAX; ++mm) o[mm] = mm < mc ? (double)v[mm][j] : 0.0;
-          if (m0 == 0) o[0] += qi[(size_t)g * C + c];
-          double *dst = q2grp + ((size_t)g * C + c) * M + m0;
-          if (mc == 4 && runs4) {
-            *(double2 *)dst = make_double2(o[0], o[1]);
-            *(double2 *)(dst + 2) = make_double2(o[2], o[3]);
-          } else {
+          for (int t = 0; t < 4; ++t)
+            if (t < nmom) tmem_ld16(tb + (uint32_t)(t * N + gb), u[t]);
+          tmem_wait_ld();
 #pragma unroll
-            for (int mm = 0; mm < MCMAX; ++mm)
-              if (mm < mc) dst[mm] = o[mm];
+          for (int j = 0; j < 16; ++j)
+            v[j] = rl == 0 ? u[0][j] : rl == 1 ? u[1][j] : rl == 2 ? u[2][j] : u[3][j];
+          if (!valid) continue;
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const int g = gb + j;
+            if (g >= G) break;
+            q2grp[((size_t)g * C + c) * M + rm] = (double)v[j] + qv[j];
           }
         }
+        fence_before_sync();
+        mbar_arrive(bar_free(tbuf));
       }
-      fence_before_sync();
-      mbar_arrive(bar_free(buf));
+      asm volatile("cp.async.wait_all;" ::: "memory");   // no copy outlives the CTA
     }
-  } else if (lane == 0) {
-    // ---- MMA issue: moment mm, material mi -> columns buf * tcols + (mm * nmat + mi) * N
+  } else if (warp == 8 && lane == 0) {
+    // ---- MMA issue: band l (every material) -> columns tbuf * tcols + l * N
     const uint32_t idesc = idesc_bf16(N);
     if (nb > 0) {
       asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_tab),
@@ -350,31 +388,49 @@ __global__ void __launch_bounds__(TC_THREADS)
     }
     bool ok = nb == 0 || mbar_wait(bar_tab, 0, err, timeout_ns);
     for (long long b = 0; ok && b < nb; ++b) {
-      const int buf = (int)(b & 1);
-      const uint32_t use = (uint32_t)(b >> 1);
-      if (!mbar_wait(bar_full(buf), use & 1u, err, timeout_ns)) break;
-      if (use > 0 && !mbar_wait(bar_free(buf), (use - 1) & 1u, err, timeout_ns)) break;
+      const int buf = (int)(b % NA), tbuf = (int)(b % TB);
+      if (!mbar_wait(bar_full(buf), (uint32_t)(b / NA) & 1u, err, timeout_ns)) break;
+      const long long tuse = b / TB;   // earlier batches on these accumulators
+      if (tuse > 0 && !mbar_wait(bar_free(tbuf), (uint32_t)(tuse - 1) & 1u, err, timeout_ns)) break;
       fence_after_sync();
-      const int m0 = (int)(b % nbt) * MC, mc = min(MC, M - m0);
-      const unsigned char *A = sA + (size_t)buf * a_buf;
-      for (int mm = 0; mm < mc; ++mm) {
-        const int k = m0 + mm;
-        int l = 0;
-        while ((l + 1) * (l + 1) <= k) ++l;
-        const uint32_t a_hi = smem_u32(A + (size_t)mm * 2 * a_tile), a_lo = a_hi + (uint32_t)a_tile;
+      for (int l = 0; l < nmom; ++l) {
+        const uint32_t d = tmem + (uint32_t)(tbuf * tcols + l * N);
         for (int mi = 0; mi < nmat; ++mi) {
-          const uint32_t d = tmem + (uint32_t)(buf * tcols + (mm * nmat + mi) * N);
+          const uint32_t a_hi = smem_u32(sA + (size_t)buf * a_buf + (size_t)mi * 2 * a_tile),
+                         a_lo = a_hi + (uint32_t)a_tile;
           const uint32_t b_hi = smem_u32(sB + ((size_t)l * nmat + mi) * 2 * b_tile),
                          b_lo = b_hi + (uint32_t)b_tile;
           for (int s = 0; s < KP / 16; ++s) {
             const uint32_t ao = (uint32_t)s * (TCR / 8) * 256, bo = (uint32_t)s * (N / 8) * 256;
-            mma_bf16(d, smem_desc(a_hi + ao), smem_desc(b_hi + bo), idesc, s > 0);
+            mma_bf16(d, smem_desc(a_hi + ao), smem_desc(b_hi + bo), idesc, mi > 0 || s > 0);
             mma_bf16(d, smem_desc(a_hi + ao), smem_desc(b_lo + bo), idesc, 1);
             mma_bf16(d, smem_desc(a_lo + ao), smem_desc(b_hi + bo), idesc, 1);
           }
         }
       }
       mma_commit(bar_mma(buf));
+    }
+  } else if (warp == 9 && lane == 0 && S > 0) {
+    // ---- loads: batch b's flux into stage b % S, one bulk copy per input group
+    for (long long b = 0; b < nb; ++b) {
+      const int st = (int)(b % S);
+      const long long use = b / S;
+      if (use > 0 && !mbar_wait(bar_rawfree(st), (uint32_t)(use - 1) & 1u, err, timeout_ns)) break;
+      if (!staged(b)) {
+        mbar_arrive(bar_raw(st));   // the converting threads load this batch themselves
+        continue;
+      }
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_raw(st)),
+                   "r"((uint32_t)stage)
+                   : "memory");
+      const unsigned char *src = (const unsigned char *)(flux + (size_t)batch_cell0(b) * M);
+      const uint32_t dst = smem_u32(sR) + (uint32_t)(st * stage);
+      for (int g = 0; g < G; ++g)
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                dst + (uint32_t)(g * run)),
+            "l"(src + (size_t)g * C * M * sizeof(double)), "r"((uint32_t)run), "r"(bar_raw(st))
+            : "memory");
     }
   }
   // every role has finished (or given up); the drain waited for the last MMAs
@@ -387,30 +443,38 @@ __global__ void __launch_bounds__(TC_THREADS)
   }
 }
 
-// Launch plan: moments per batch MC (the largest of 4, 2, 1 whose
-// accumulators, MC * nmat tiles of N columns, fit the 512 tensor-memory
-// columns and whose operands fit 200 KB of shared memory), the tensor-memory
-// columns to allocate (a power of two >= 32) and the shared-memory bytes.
+// Launch plan: accumulator sets (TB = 2 when two sets of nmom tiles of N
+// columns fit the 512 tensor-memory columns, else 1), the columns to
+// allocate (a power of two >= 32), the flux stages (as many as fit, at most
+// TC_MAX_STAGES; none when the per-group runs are not 16-byte aligned) and
+// the shared-memory bytes (scattering operands, NA operand buffers, stages).
 struct TcPlan {
-  int N, KP, MC, cols;
+  int N, KP, NA, TB, S, cols;
   size_t smem;
 };
 
-bool tc_plan(int G, int nmat, int nmom, TcPlan *pl) {
+bool tc_plan(int G, int nmat, int nmom, long long C, TcPlan *pl) {
+  const int M = nmom * nmom;
   pl->N = pad16(G);
   pl->KP = pad16(G);
-  const size_t b_bytes = (size_t)nmom * nmat * 2 * pl->N * pl->KP * 2;
-  for (int mc = MCMAX; mc >= 1; mc /= 2) {
-    const size_t smem = b_bytes + 2 * (size_t)mc * 2 * TCR * pl->KP * 2;   // two operand buffers
-    if (2LL * mc * nmat * pl->N <= 512 && smem <= 220 * 1024) {            // two accumulator buffers
-      pl->MC = mc;
-      pl->smem = smem;
-      pl->cols = 32;
-      while (pl->cols < 2 * mc * nmat * pl->N) pl->cols <<= 1;
-      return true;
-    }
-  }
-  return false;
+  const long long tcols = (long long)nmom * pl->N;
+  if (tcols > 512 || M > TCR || nmom > 4) return false;
+  pl->TB = 2 * tcols <= 512 ? 2 : 1;
+  pl->cols = 32;
+  while (pl->cols < pl->TB * tcols) pl->cols <<= 1;
+  const size_t b_bytes = (size_t)nmom * nmat * 2 * pl->N * pl->KP * 2,
+               a_buf = (size_t)nmat * 2 * TCR * pl->KP * 2;
+  const size_t q_bytes = 2 * (size_t)(TCR / M) * G * sizeof(double);   // two batches' qi
+  pl->NA = b_bytes + 2 * a_buf + q_bytes <= 200 * 1024 ? 2 : 1;   // operand buffers
+  const size_t base = b_bytes + pl->NA * a_buf + q_bytes;
+  if (base > 200 * 1024) return false;
+  const size_t run = (size_t)(TCR / M) * M * sizeof(double), stage = run * G;
+  const bool aligned = run % 16 == 0 && (C * M * sizeof(double)) % 16 == 0;
+  pl->S = 0;
+  while (aligned && pl->S < TC_MAX_STAGES && base + (pl->S + 1) * stage <= 200 * 1024) ++pl->S;
+  if (pl->S == 1) pl->S = 0;   // one stage would not run ahead
+  pl->smem = base + pl->S * stage;
+  return true;
 }
 
 }  // namespace
@@ -422,20 +486,17 @@ size_t outer_tc_table_words(int G, int nmat, int nmom) {
 
 bool outer_tc_supported(int G, int nmat, int nmom) {
   TcPlan pl;
-  return tc_plan(G, nmat, nmom, &pl);
+  return tc_plan(G, nmat, nmom, 2, &pl);
 }
 
-bool outer_tc_preferred(int G, int nmat, int nmom) {
-  TcPlan pl;
-  return tc_plan(G, nmat, nmom, &pl) && pl.MC == MCMAX;
-}
+bool outer_tc_preferred(int G, int nmat, int nmom) { return outer_tc_supported(G, nmat, nmom); }
 
 cudaError_t k_outer_source_tc(const double *qi, const double *slgg, const int32_t *mat,
                               const double *flux, double *q2grp, uint32_t *tab, int G, int nmat,
                               int nmom, int M, long long C, int *err, long long timeout_ns,
                               cudaStream_t st) {
   TcPlan pl;
-  if (!tc_plan(G, nmat, nmom, &pl)) return cudaErrorInvalidValue;
+  if (!tc_plan(G, nmat, nmom, C, &pl)) return cudaErrorInvalidValue;
   tcb_table_kernel<<<64, 256, 0, st>>>(slgg, G, nmat, nmom, pl.N, pl.KP, (__nv_bfloat16 *)tab);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
@@ -458,11 +519,11 @@ cudaError_t k_outer_source_tc(const double *qi, const double *slgg, const int32_
   const int by_smem = (int)((size_t)smem_sm / (pl.smem + 2048));
   const int by_regs = 65536 / (((fa.numRegs + 7) / 8 * 8) * TC_THREADS);
   const int blocks = std::max(1, std::min(std::min(by_smem, 512 / pl.cols), by_regs));
-  const long long tiles = (C + TCR - 1) / TCR;
-  const int grid = (int)std::min<long long>(tiles, (long long)blocks * sms);
+  const long long batches = (C + TCR / M - 1) / (TCR / M);
+  const int grid = (int)std::min<long long>(batches, (long long)blocks * sms);
   outer_source_tc_kernel<<<grid, TC_THREADS, pl.smem, st>>>(qi, (const __nv_bfloat16 *)tab, mat, flux,
-                                                     q2grp, G, pl.N, pl.KP, nmat, nmom, M, pl.MC,
-                                                     C, pl.cols, err, timeout_ns);
+                                                     q2grp, G, pl.N, pl.KP, nmat, nmom, M, pl.NA, pl.TB,
+                                                     pl.S, C, pl.cols, err, timeout_ns);
   return cudaGetLastError();
 }
 
