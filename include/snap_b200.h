@@ -151,8 +151,10 @@ int snap_sweep(snap_ctx *ctx, const void *qtot, const void *t_xs, void *flux, vo
  * its own flag), and qim added to the angular source when not NULL; groups
  * with vdelt == 0 sweep as in steady state.  vdelt [ng]; psi_t_in,
  * psi_t_out and qim [octant][g][c][nang]; all device, FP64 contexts.  Runs
- * the general sweep kernel.  Replaces run_gpu_sweep with time dependence
- * (gpu_sweep.cu:738-1393). */
+ * the tiled kernel's time-dependent form where the context has one flux
+ * moment and a tiled shape (at most 64 angles), else the general kernel
+ * (SNAP_B200_TD_GENERAL=1 selects the general kernel always).  Replaces
+ * run_gpu_sweep with time dependence (gpu_sweep.cu:738-1393). */
 int snap_sweep_td(snap_ctx *ctx, const double *qtot, const double *t_xs, const double *vdelt,
                   const double *psi_t_in, double *psi_t_out, const double *qim, double *flux,
                   void *stream);
@@ -262,8 +264,9 @@ typedef struct {
  * fourth outgoing face (with its own fixup flag), the two halves of psi_t
  * swapping roles every step.  Replaces Snap::transport_solve with
  * time_dependent = true (snap.cc:409-541, sweep.cc:413-419, 461-468, 473-518).
- * The sweep is the general kernel (any mesh, up to 2048 angles per octant).
- * FP64 contexts.  info->inners_per_outer lists the outer iterations of all
+ * The sweep is that of snap_sweep_td (the tiled kernel for one moment and
+ * at most 64 angles, else the general kernel: any mesh, up to 2048 angles
+ * per octant).  FP64 contexts.  info->inners_per_outer lists the outer iterations of all
  * steps in order. */
 int snap_transport_solve_td(snap_ctx *ctx, const int32_t *mat, const double *qi,
                             const double *sigt, const double *slgg, const double *sigt_scale,

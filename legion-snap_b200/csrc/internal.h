@@ -46,6 +46,13 @@ struct SweepParams {
   uint8_t *flag_store;    // [8][G][C][AP]
   // Adjoint sweep only: the adjoint of t_xs per octant slot, [P][G][C].
   void *sigt_bar_slots;
+  // Time-dependent form only (FP64, one moment; null otherwise): vdelt [G]
+  // and per (octant, group, cell, angle) the time-edge flux in and out and
+  // the manufactured source (may be null), [8][G][C][A].
+  const double *vdelt;
+  const double *tf_in;
+  double *tf_out;
+  const double *qim;
 };
 
 // Parameters of the general sweep (sweep_wide.cu): one CTA per (octant,
@@ -109,6 +116,10 @@ int set_last_error(int code, const std::string &msg);
 enum : int { DEV_ERR_NONE = 0, DEV_ERR_TIMEOUT = 1 };
 
 // sweep kernels (sweep_fp64.cu / sweep_fp32.cu)
+// the time-dependent form of the tiled kernel (FP64, one moment: MK = 0)
+cudaError_t launch_sweep_fp64_td(const SweepShape &sh, const SweepParams &p, int grid,
+                                 cudaStream_t st);
+cudaError_t sweep_fp64_td_occupancy(const SweepShape &sh, int *blocks_per_sm, size_t *smem);
 cudaError_t launch_sweep_fp64(const SweepShape &sh, const SweepParams &p, int grid,
                               cudaStream_t st);
 cudaError_t sweep_fp64_occupancy(const SweepShape &sh, int *blocks_per_sm, size_t *smem);

@@ -65,6 +65,7 @@ struct snap_ctx {
   // FP32 contexts: the split-TF32 tensor-core sweep over group pairs
   int tc32 = 0;
   int n_pair_items = 0, grid_tc = 0;
+  int grid_td = 0;   // CTAs of the time-dependent tiled sweep (0: not yet sized)
   int *d_pair_table = nullptr, *d_pair_index = nullptr;
   void *d_tc1 = nullptr, *d_tc2 = nullptr;
   uint32_t *d_scat_tc = nullptr;   // BF16 scattering fragments of the tensor-core outer source
@@ -297,13 +298,30 @@ void build_items(int P, int G, int tx_n, int ty_n, std::vector<int> &table,
       }
 }
 
+// Time-dependent terms of one inner iteration's sweep.
+struct TdArgs {
+  const double *vdelt;   // [G]
+  const double *tf_in;   // [8][G][C][A]
+  double *tf_out;        // [8][G][C][A]
+  const double *qim;     // [8][G][C][A] or null
+};
+
+// Whether the time-dependent sweep runs on the tiled kernel: FP64 contexts
+// with one flux moment whose shape the tiled kernel takes (at most 64
+// angles); SNAP_B200_TD_GENERAL=1 sends it to the general kernel.
+bool td_tiled(const snap_ctx *c) {
+  if (const char *e = getenv("SNAP_B200_TD_GENERAL"))
+    if (atoi(e) != 0) return false;
+  return !c->wide_only && !c->fp32 && !c->tc32 && c->shape.MK == 0;
+}
+
 // mode 0: forward sweep; 1: forward sweep recording the state for the
 // adjoint; 2: adjoint sweep (sigma_t adjoint when sbar != null).
 // With atomic_flux (forward mode only), every octant adds its moments into
 // that FP64 flux [G][C][cmom] instead of writing its slot.
 int sweep_launches(snap_ctx *c, const void *qtot, const void *t_xs, cudaStream_t st,
                    int mode = 0, void *sbar = nullptr, double *atomic_flux = nullptr,
-                   int g0 = 0, int gn = 0) {
+                   int g0 = 0, int gn = 0, const TdArgs *td = nullptr) {
   // gn > 0: only groups g0 .. g0+gn-1 (qtot and t_xs hold every group; the
   // slots, the recorded state and sbar hold the batch)
   const bool batch = gn > 0 && gn < c->cfg.ng;
@@ -358,6 +376,22 @@ int sweep_launches(snap_ctx *c, const void *qtot, const void *t_xs, cudaStream_t
   p.flag_store = mode >= 1 ? c->d_flag_store : nullptr;
   p.sigt_bar_slots = mode == 2 ? sbar : nullptr;
   int grid = c->grid;
+  if (td) {   // the time-dependent form: every octant adds into the FP64 flux
+    if (!atomic_flux || mode != 0 || batch) return fail(SNAP_ERR_BAD_ARG, "time-dependent sweep");
+    p.vdelt = td->vdelt;
+    p.tf_in = td->tf_in;
+    p.tf_out = td->tf_out;
+    p.qim = td->qim;
+    if (c->grid_td == 0) {
+      int blocks = 0, sms = 0;
+      size_t smem = 0;
+      if (sweep_fp64_td_occupancy(c->shape, &blocks, &smem) != cudaSuccess || blocks < 1)
+        return fail(SNAP_ERR_UNSUPPORTED, "time-dependent tiled sweep does not fit on the device");
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+      c->grid_td = std::min(blocks * sms, c->n_items);
+    }
+    grid = c->grid_td;
+  }
   const bool tc = c->tc32 && mode != 2;
   if (tc) {
     p.n_items = c->n_pair_items;
@@ -382,7 +416,9 @@ int sweep_launches(snap_ctx *c, const void *qtot, const void *t_xs, cudaStream_t
     p.accumulate = L > 0;
     SNAP_CUDA(cudaMemsetAsync(c->d_ctrl, 0, sizeof(int) * (c->n_progress() + 1), st));
     cudaError_t e;
-    if (mode == 2)
+    if (td)
+      e = launch_sweep_fp64_td(c->shape, p, grid, st);
+    else if (mode == 2)
       e = adjoint_dispatch(c->fp32, c->shape, 0, &p, grid, st, nullptr, nullptr);
     else if (tc)
       e = launch_sweep_tc32(c->shape, p, grid, st);
@@ -428,13 +464,6 @@ int read_ctrl(snap_ctx *c, cudaStream_t st, int *violations) {
   return SNAP_OK;
 }
 
-// Time-dependent terms of one inner iteration's sweep.
-struct TdArgs {
-  const double *vdelt;   // [G]
-  const double *tf_in;   // [8][G][C][A]
-  double *tf_out;        // [8][G][C][A]
-  const double *qim;     // [8][G][C][A] or null
-};
 int inner_iteration_impl(snap_ctx *c, const double *s_xs, const double *q2grp, const void *t_xs,
                          double *flux, void *qtot, double epsi, int *converged, cudaStream_t st,
                          const TdArgs *td);
@@ -877,7 +906,9 @@ int snap_sweep_td(snap_ctx *c, const double *qtot, const double *t_xs, const dou
   SNAP_CUDA(cudaMemsetAsync(c->error(), 0, 2 * sizeof(int), st));
   SNAP_CUDA(cudaMemsetAsync(flux, 0, sizeof(double) * c->cfg.ng * c->C * c->M, st));
   SNAP_CUDA(cudaEventRecord(c->sw0, st));
-  int rc = wide_sweep(c, qtot, t_xs, flux, vdelt, psi_t_in, psi_t_out, qim, st);
+  const TdArgs td{vdelt, psi_t_in, psi_t_out, qim};
+  int rc = td_tiled(c) ? sweep_launches(c, qtot, t_xs, st, 0, nullptr, flux, 0, 0, &td)
+                       : wide_sweep(c, qtot, t_xs, flux, vdelt, psi_t_in, psi_t_out, qim, st);
   if (rc) return rc;
   SNAP_CUDA(cudaEventRecord(c->sw1, st));
   rc = read_ctrl(c, st, nullptr);
@@ -898,8 +929,8 @@ int snap_inner_iteration(snap_ctx *c, const double *s_xs, const double *q2grp, c
 namespace {
 
 // The inner-loop body (snap.cc:487-503).  td != null: the time-dependent
-// sweep of the general kernel (vdelt, the time-edge angular flux, the
-// manufactured source).
+// sweep (vdelt, the time-edge angular flux, the manufactured source) on the
+// tiled kernel where td_tiled() allows, else on the general kernel.
 int inner_iteration_impl(snap_ctx *c, const double *s_xs, const double *q2grp, const void *t_xs,
                          double *flux, void *qtot, double epsi, int *converged, cudaStream_t st,
                          const TdArgs *td) {
@@ -910,7 +941,18 @@ int inner_iteration_impl(snap_ctx *c, const double *s_xs, const double *q2grp, c
   constexpr double kFp32InnerFloor = 32.0 / 16777216.0;
   const double eps_in = c->fp32 ? std::max(epsi, kFp32InnerFloor) : epsi;
   int rc = SNAP_OK;
-  if (c->wide_only || td) {
+  if (td && td_tiled(c)) {
+    // the time-dependent form of the tiled kernel, octants added into the flux
+    SNAP_CUDA(k_inner_source_save(s_xs, q2grp, flux, qtot, 0, c->d_old0, c->cfg.ng, c->cfg.nmom,
+                                  c->M, c->C, st));
+    SNAP_CUDA(cudaEventRecord(c->sw0, st));
+    rc = sweep_launches(c, qtot, t_xs, st, 0, nullptr, flux, 0, 0, td);
+    if (rc) return rc;
+    SNAP_CUDA(cudaEventRecord(c->sw1, st));
+    SNAP_CUDA(k_test_change(flux, c->d_old0, c->M, (long long)c->cfg.ng * c->C, eps_in,
+                            c->violations(), c->maxdf(), st));
+    c->launches += 2;
+  } else if (c->wide_only || td) {
     SNAP_CUDA(k_inner_source_save(s_xs, q2grp, flux, qtot, 0, c->d_old0, c->cfg.ng, c->cfg.nmom,
                                   c->M, c->C, st));
     SNAP_CUDA(cudaEventRecord(c->sw0, st));

@@ -48,6 +48,15 @@ cudaError_t launch_sweep_fp64(const SweepShape &sh, const SweepParams &p, int gr
                               cudaStream_t st) {
   return dispatch(kFp64, sh, 0, &p, grid, st, nullptr, nullptr);
 }
+cudaError_t launch_sweep_fp64_td(const SweepShape &sh, const SweepParams &p, int grid,
+                                 cudaStream_t st) {
+  if (!supported(sh) || sh.MK != 0) return cudaErrorInvalidValue;
+  return kFp64[sh.NT](-1, sh.TY, 0, &p, grid, st, nullptr, nullptr);
+}
+cudaError_t sweep_fp64_td_occupancy(const SweepShape &sh, int *blocks_per_sm, size_t *smem) {
+  if (!supported(sh) || sh.MK != 0) return cudaErrorInvalidValue;
+  return kFp64[sh.NT](-1, sh.TY, 1, nullptr, 0, nullptr, blocks_per_sm, smem);
+}
 cudaError_t launch_sweep_fp32(const SweepShape &sh, const SweepParams &p, int grid,
                               cudaStream_t st) {
   return dispatch(kFp32, sh, 0, &p, grid, st, nullptr, nullptr);
