@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "device_util.cuh"
 #include "internal.h"
@@ -36,8 +37,10 @@ constexpr unsigned FULL = 0xffffffffu;
 constexpr int MAX_THREADS = 512;
 constexpr int MAX_WARPS = MAX_THREADS / 32;
 
-template <int APT>
-__global__ void __launch_bounds__(MAX_THREADS) wide_sweep_kernel(const WideParams p) {
+// MAXT: the CTA size the register budget is sized for (128 threads leave
+// room for four angles per thread without spilling).
+template <int APT, int MAXT>
+__global__ void __launch_bounds__(MAXT) wide_sweep_kernel(const WideParams p) {
   extern __shared__ double s_red[];   // [warps][nx][M] per-warp moment partials of a pencil
   __shared__ int s_cnt[MAX_WARPS];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -245,7 +248,19 @@ __global__ void __launch_bounds__(MAX_THREADS) wide_sweep_kernel(const WideParam
 
 }  // namespace
 
-int wide_apt(int A) { return A > 2 * MAX_THREADS ? 4 : A > MAX_THREADS ? 2 : 1; }
+// Angles per thread: enough for a CTA of at most 128 threads where four per
+// thread suffice (fewer warps shorten the per-cell barrier and reductions:
+// on the 4096-cell reference decks, 256 angles 8.3 -> 5.2 ms per sweep and
+// 512 angles 18.9 -> 12.5 ms against one angle per thread), else four; more
+// when SNAP_B200_WIDE_APT asks (2 or 4).
+int wide_apt(int A) {
+  int apt = A <= 128 ? 1 : A <= 256 ? 2 : 4;
+  if (const char *e = getenv("SNAP_B200_WIDE_APT")) {
+    const int want = atoi(e);
+    if (want == 2 || want == 4) apt = std::max(apt, want);
+  }
+  return apt;
+}
 
 int wide_threads(int A) {
   const int apt = wide_apt(A);
@@ -262,13 +277,13 @@ bool wide_supported(int A, int nx, int M) {
          wide_smem_bytes(A, nx, M) <= 200 * 1024;
 }
 
-template <int APT>
+template <int APT, int MAXT>
 cudaError_t launch_apt(const WideParams &p, int n_blocks, int threads, size_t smem,
                        cudaStream_t st) {
-  cudaError_t e = cudaFuncSetAttribute(wide_sweep_kernel<APT>,
+  cudaError_t e = cudaFuncSetAttribute(wide_sweep_kernel<APT, MAXT>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  wide_sweep_kernel<APT><<<n_blocks, threads, smem, st>>>(p);
+  wide_sweep_kernel<APT, MAXT><<<n_blocks, threads, smem, st>>>(p);
   return cudaGetLastError();
 }
 
@@ -276,10 +291,16 @@ cudaError_t launch_sweep_wide(const WideParams &p, int n_blocks, cudaStream_t st
   if (!wide_supported(p.A, p.nx, p.M)) return cudaErrorInvalidValue;
   const int threads = wide_threads(p.A);
   const size_t smem = wide_smem_bytes(p.A, p.nx, p.M);
+  // register budgets: 255 per thread up to 256 threads, 128 beyond
   switch (wide_apt(p.A)) {
-    case 1: return launch_apt<1>(p, n_blocks, threads, smem, st);
-    case 2: return launch_apt<2>(p, n_blocks, threads, smem, st);
-    default: return launch_apt<4>(p, n_blocks, threads, smem, st);
+    case 1: return launch_apt<1, MAX_THREADS>(p, n_blocks, threads, smem, st);
+    case 2:
+      return threads <= 128 ? launch_apt<2, 128>(p, n_blocks, threads, smem, st)
+                            : launch_apt<2, MAX_THREADS>(p, n_blocks, threads, smem, st);
+    default:
+      return threads <= 128   ? launch_apt<4, 128>(p, n_blocks, threads, smem, st)
+             : threads <= 256 ? launch_apt<4, 256>(p, n_blocks, threads, smem, st)
+                              : launch_apt<4, MAX_THREADS>(p, n_blocks, threads, smem, st);
   }
 }
 
