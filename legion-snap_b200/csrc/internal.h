@@ -77,11 +77,19 @@ struct WideParams {
   double *flux;                      // [G][C][M], every octant added atomically
   double *ypen;                      // scratch [blocks][nx][A]
   double *zpl;                       // scratch [blocks][ny*nx][A]
+  // face planes of the wavefront form (sweep_wave.cu)
+  double *wx;                        // scratch [blocks][ny*nz][A]
+  double *wy;                        // scratch [blocks][nx*nz][A]
+  double *wz;                        // scratch [blocks][nx*ny][A]
 };
 int wide_threads(int A);
 size_t wide_smem_bytes(int A, int nx, int M);
 bool wide_supported(int A, int nx, int M);
 cudaError_t launch_sweep_wide(const WideParams &p, int n_blocks, cudaStream_t st);
+// the wavefront form of the general sweep: up to 128 angles per octant
+bool wave_supported(int A, int M);
+size_t wave_scratch_doubles(int nx, int ny, int nz, int A, int blocks);
+cudaError_t launch_sweep_wave(const WideParams &p, int n_blocks, cudaStream_t st);
 
 // The manufactured-solution check (mms.cu).
 struct MmsGeometry {

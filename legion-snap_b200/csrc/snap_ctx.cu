@@ -85,7 +85,9 @@ struct snap_ctx {
   // (ragged meshes, more than 64 angles) and every time-dependent sweep
   bool wide_only = false;       // the tiled kernel cannot run this shape
   double *d_wquad = nullptr;    // [mu, eta, xi, w: 4*A][ec: 8*M*A]
-  double *d_wscratch = nullptr; // y pencils and z planes of 8*G blocks
+  double *d_wscratch = nullptr; // general sweep: y pencils and z planes of 8*G blocks, or
+                                // the x, y and z face planes of the wavefront form
+  bool wave = false;            // the general sweep runs in its wavefront form
   double *d_vdelt0 = nullptr;   // [G] zeros: steady-state vdelt
   double *d_vdelt = nullptr;    // [G] vdelt of the current time-dependent solve
   std::vector<double> h_vdelt;
@@ -476,7 +478,18 @@ int solve_impl(snap_ctx *c, const int32_t *mat, const double *qi, const double *
 int ensure_wide(snap_ctx *c) {
   if (c->d_wscratch) return SNAP_OK;
   const int A = c->A, M = c->M, G = c->cfg.ng;
-  if (!wide_supported(A, c->cfg.nx, M))
+  // the wavefront form where it takes the shape and its face planes fit in
+  // a quarter of the free memory (SNAP_B200_WAVE=0: the cell-by-cell form)
+  bool wave = wave_supported(A, M);
+  if (const char *e = getenv("SNAP_B200_WAVE"))
+    if (atoi(e) == 0) wave = false;
+  const size_t wave_bytes =
+      sizeof(double) * wave_scratch_doubles(c->cfg.nx, c->cfg.ny, c->cfg.nz, A, 8 * G);
+  if (wave) {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess || wave_bytes > free_b / 4) wave = false;
+  }
+  if (!wave && !wide_supported(A, c->cfg.nx, M))
     return fail(SNAP_ERR_UNSUPPORTED, "no general sweep for this shape");
   std::vector<double> q((size_t)4 * A + (size_t)8 * M * A);
   for (int a = 0; a < A; ++a) {
@@ -489,7 +502,7 @@ int ensure_wide(snap_ctx *c) {
   int rc = upload((void **)&c->d_wquad, q);
   if (rc) return rc;
   const size_t per_block = (size_t)c->cfg.nx * (1 + c->cfg.ny) * A;
-  const size_t bytes = sizeof(double) * per_block * 8 * G;
+  const size_t bytes = wave ? wave_bytes : sizeof(double) * per_block * 8 * G;
   if (cudaMalloc((void **)&c->d_wscratch, bytes) != cudaSuccess ||
       cudaMalloc((void **)&c->d_vdelt0, sizeof(double) * G) != cudaSuccess ||
       cudaMemset(c->d_vdelt0, 0, sizeof(double) * G) != cudaSuccess) {
@@ -499,6 +512,7 @@ int ensure_wide(snap_ctx *c) {
     return fail(SNAP_ERR_OOM, "cannot allocate the general sweep's face scratch");
   }
   c->scratch_bytes += bytes + sizeof(double) * G;
+  c->wave = wave;
   return SNAP_OK;
 }
 
@@ -536,9 +550,17 @@ int wide_sweep(snap_ctx *c, const double *qtot, const double *t_xs, double *flux
   p.tf_out = tf_out;
   p.qim = qim;
   p.flux = flux;
-  p.ypen = c->d_wscratch;
-  p.zpl = c->d_wscratch + (size_t)c->cfg.nx * A * 8 * G;
-  SNAP_CUDA(launch_sweep_wide(p, 8 * G, st));
+  if (c->wave) {
+    const size_t blocks = (size_t)8 * G;
+    p.wx = c->d_wscratch;
+    p.wy = p.wx + (size_t)c->cfg.ny * c->cfg.nz * A * blocks;
+    p.wz = p.wy + (size_t)c->cfg.nx * c->cfg.nz * A * blocks;
+    SNAP_CUDA(launch_sweep_wave(p, 8 * G, st));
+  } else {
+    p.ypen = c->d_wscratch;
+    p.zpl = c->d_wscratch + (size_t)c->cfg.nx * A * 8 * G;
+    SNAP_CUDA(launch_sweep_wide(p, 8 * G, st));
+  }
   ++c->launches;
   return SNAP_OK;
 }

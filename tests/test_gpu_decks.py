@@ -136,6 +136,39 @@ def test_task_level_time_dependent_sweep_fixups(monkeypatch):
     snap.close()
 
 
+@pytest.mark.parametrize("case", ["small_512_1x1x1.in", "ragged_nmom3", "ragged_fixup"])
+def test_wavefront_general_sweep_matches_cell_by_cell(case, monkeypatch):
+    """The general sweep's wavefront form (the cells of a diagonal plane in
+    flight at once, one warp per cell; up to 128 angles) against its
+    cell-by-cell form (SNAP_B200_WAVE=0) on whole solves: the 128-angle
+    time-dependent deck, a ragged mesh with nmom = 3, and a ragged
+    fixup-heavy mesh; flux to 1e-12 and identical iteration records."""
+    from snap_b200.solver import Snap
+    if case.endswith(".in"):
+        d = D.parse_deck(DECKS / case).deck
+        d = dataclasses.replace(d, nsteps=2, tf=2 * d.dt)
+    elif case == "ragged_nmom3":
+        d = P.Deck(12, 10, 6, nang=40, ng=3, nmom=3, epsi=1e-6, iitm=3, oitm=3)
+    else:
+        d = P.Deck(9, 7, 5, nang=96, ng=2, nmom=1, epsi=1e-6, iitm=3, oitm=3, lx=8.0, ly=8.0,
+                   lz=8.0)
+
+    def run():
+        snap = Snap(d)
+        flux, rec = snap.transport_solve(snap.device_problem(P.make_problem(d)))
+        snap.close()
+        return flux.cpu().numpy(), rec
+
+    wave, rw = run()
+    monkeypatch.setenv("SNAP_B200_WAVE", "0")
+    cell, rc = run()
+    assert rel_err(wave[..., 0], cell[..., 0]) < TOL
+    if d.cmom > 1:
+        scale = np.abs(cell).reshape(-1, d.cmom).max(axis=0)
+        assert float((np.abs(wave - cell).reshape(-1, d.cmom).max(axis=0) / scale).max()) < TOL
+    assert rw["inners_per_outer"] == rc["inners_per_outer"]
+
+
 @needs_ref
 def test_time_dependent_2048_angles():
     """The largest angle count the general kernel takes (four angles per
