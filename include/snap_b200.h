@@ -67,7 +67,10 @@ typedef struct snap_ctx snap_ctx;
  * slots, tile-boundary faces, progress flags).  Shapes outside the tiled
  * sweep kernel (nx not a multiple of 8, ny not a multiple of 4, more than 64
  * angles per octant) run every forward sweep on the general kernel (one CTA
- * per octant and group, up to 2048 angles; FP64 contexts only; no adjoint).
+ * per octant and group; up to 128 angles the cells of a diagonal plane in
+ * flight, one warp per cell, else cell by cell up to 2048 angles; FP64
+ * contexts only; no adjoint).  SNAP_B200_WAVE=0 selects the cell-by-cell
+ * form always.
  * Replaces InitGPUSweep -> initialize_gpu_context (init.cc:215-236,
  * gpu_sweep.cu:71-273). */
 int snap_create(const snap_config *cfg, int device, snap_ctx **out);
