@@ -38,3 +38,40 @@ def test_python_binding_covers_header():
     sys.path.insert(0, str(ROOT / "legion-snap_b200"))
     from snap_b200 import abi
     assert set(declared_symbols()) <= set(abi.SIGNATURES)
+
+
+# entry points that take a context first; called with a null context (and
+# null or zero for everything else) each returns SNAP_ERR_BAD_ARG with a
+# message, before touching a device
+NULL_CTX_EXEMPT = {
+    "snap_create", "snap_destroy", "snap_scratch_bytes", "snap_sweep_noalloc",
+    "snap_selftest_division", "snap_last_error",
+}
+
+
+@pytest.mark.skipif(not LIB.exists(), reason="library not built")
+def test_null_context_is_rejected():
+    import sys
+    sys.path.insert(0, str(ROOT / "legion-snap_b200"))
+    from snap_b200 import abi
+    lib = abi.load()
+    for name, argtypes in abi.SIGNATURES.items():
+        if name in NULL_CTX_EXEMPT:
+            continue
+        args = [0.0 if t is ctypes.c_double else 0 if t in (ctypes.c_int, ctypes.c_longlong)
+                else None for t in argtypes]
+        rc = getattr(lib, name)(*args)
+        assert abi.STATUS.get(rc) == "SNAP_ERR_BAD_ARG", (name, rc)
+        assert lib.snap_last_error(), name
+
+
+@pytest.mark.skipif(not LIB.exists(), reason="library not built")
+def test_create_rejects_null_arguments():
+    import sys
+    sys.path.insert(0, str(ROOT / "legion-snap_b200"))
+    from snap_b200 import abi
+    lib = abi.load()
+    h = ctypes.c_void_p()
+    assert abi.STATUS.get(lib.snap_create(None, 0, ctypes.byref(h))) == "SNAP_ERR_BAD_ARG"
+    assert abi.STATUS.get(lib.snap_create(None, 0, None)) == "SNAP_ERR_BAD_ARG"
+    assert lib.snap_destroy(None) in (0, 1)   # destroying nothing is harmless
