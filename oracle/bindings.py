@@ -111,6 +111,16 @@ class Oracle:
         self.lib.oracle_sweep(C.byref(self.geom), _d(qtot), _d(t_xs), _d(flux))
         return flux
 
+    def adjoint_sweep(self, qtot, t_xs, phi_bar):
+        """The transpose of sweep() at the forward state of qtot (fixup flags
+        frozen): (qtot_bar [G][C][cmom], sigt_bar [G][C])."""
+        d = self.deck
+        qb = np.zeros((d.ng, self.C, d.cmom))
+        sb = np.zeros((d.ng, self.C))
+        self.lib.oracle_adjoint_sweep(C.byref(self.geom), _d(qtot), _d(t_xs), _d(phi_bar), _d(qb),
+                                      _d(sb))
+        return qb, sb
+
     def test_convergence(self, flux, prev, epsi):
         self.lib.oracle_test_convergence.restype = C.c_int
         return bool(self.lib.oracle_test_convergence(C.byref(self.geom), _d(flux), _d(prev),

@@ -297,6 +297,181 @@ void oracle_sweep(const oracle_geom *g, const double *qtot, const double *t_xs,
   par_for(g->ng, sweep_group, &x);   /* groups: snap.cc:872; octants in order: :865 */
 }
 
+/* Adjoint of one (octant, group) sweep with the fixup flags frozen at the
+ * forward state (no reference counterpart; the transpose of
+ * oracle_sweep_octant_group): a forward pass over the cells in upwind order
+ * records, per cell and angle, pc, the face flags the last fixup recompute
+ * used (p_d), the flags of the outgoing faces (h_d), and whether pc was set
+ * to zero; the reverse pass walks the cells downstream-first with the
+ * adjoint faces and adds
+ *   pc_bar   = sum_k ec[k][a] w[a] phi_bar[k] + 2 sum_d h_d out_bar_d
+ *   s        = pc_bar / den          (0 where pc was set to zero)
+ *   in_bar_d = -h_d out_bar_d + s (1 + p_d) c_d / 2
+ *   qtot_bar[k] += ec[k][a] s,  sigt_bar -= s pc
+ * where pc = (psi + sum_d c_d in_d (1 + p_d) / 2) / (sigma_t + sum_d c_d p_d)
+ * (all p_d = 1: the diamond difference) and out_d = (2 pc - in_d) h_d. */
+void oracle_adjoint_octant_group(const oracle_geom *g, int corner, int group,
+                                 const double *qtot, const double *t_xs,
+                                 const double *phi_bar, double *qtot_bar,
+                                 double *sigt_bar) {
+  const int nx = g->nx, ny = g->ny, nz = g->nz, A = g->nang, cmom = g->cmom;
+  const size_t C = (size_t)nx * ny * nz;
+  const int sx = (corner & 1) != 0, sy = (corner & 2) != 0, sz = (corner & 4) != 0;
+  const double tolr = 1.0e-12;
+  const double *ec = g->ec + (size_t)corner * cmom * A;
+  /* recorded forward state, indexed by the cell's position in sweep order */
+  double *rpc = (double *)calloc(C * A, sizeof(double));
+  double *rden = (double *)calloc(C * A, sizeof(double));
+  unsigned char *rflag = (unsigned char *)calloc(C * A, 1);   /* p x,y,z bits 0-2, h bits 3-5, zero bit 6 */
+  double *buf = (double *)calloc((size_t)A * 14 + (size_t)A * nx + (size_t)A * nx * ny, sizeof(double));
+  double *psi = buf, *pc = psi + A, *psii = pc + A, *psij = psii + A, *psik = psij + A;
+  double *hv_x = psik + A, *hv_y = hv_x + A, *hv_z = hv_y + A;
+  double *fx = hv_z + A, *fy = fx + A, *fz = fy + A, *pvx = fz + A, *pvy = pvx + A, *pvz = pvy + A;
+  double *ypencil = pvz + A, *zplane = ypencil + (size_t)A * nx;
+  unsigned char *zero = (unsigned char *)calloc(A, 1);
+  size_t n = 0;   /* cell position in sweep order */
+  for (int zz = 0; zz < nz; zz++) {
+    const int z = sz ? zz : nz - 1 - zz;
+    for (int yy = 0; yy < ny; yy++) {
+      const int y = sy ? yy : ny - 1 - yy;
+      for (int xx = 0; xx < nx; xx++, n++) {
+        const int x = sx ? xx : nx - 1 - xx;
+        const size_t c = ((size_t)z * ny + y) * nx + x;
+        const double *q = qtot + (group * C + c) * cmom;
+        const double sig = t_xs[group * C + c];
+        for (int a = 0; a < A; a++) psi[a] = q[0];
+        for (int k = 1; k < cmom; k++)
+          for (int a = 0; a < A; a++) psi[a] += ec[(size_t)k * A + a] * q[k];
+        if (xx == 0) memset(psii, 0, sizeof(double) * A);
+        if (yy == 0) memset(psij, 0, sizeof(double) * A);
+        else memcpy(psij, ypencil + (size_t)xx * A, sizeof(double) * A);
+        if (zz == 0) memset(psik, 0, sizeof(double) * A);
+        else memcpy(psik, zplane + ((size_t)yy * nx + xx) * A, sizeof(double) * A);
+        for (int a = 0; a < A; a++) {
+          const double den = sig + g->hi * g->mu[a] + g->hj * g->eta[a] + g->hk * g->xi[a];
+          pc[a] = (psi[a] + psii[a] * g->mu[a] * g->hi + psij[a] * g->eta[a] * g->hj +
+                   psik[a] * g->xi[a] * g->hk) / den;
+          rden[n * A + a] = den;
+          hv_x[a] = hv_y[a] = hv_z[a] = 1.0;
+          pvx[a] = pvy[a] = pvz[a] = 1.0;
+          zero[a] = 0;
+        }
+        if (g->fixup) {
+          unsigned old_neg = 0;
+          for (;;) {
+            unsigned neg = 0;
+            for (int a = 0; a < A; a++) {
+              fx[a] = 2.0 * pc[a] - psii[a];
+              if (fx[a] < 0.0) { hv_x[a] = 0.0; neg++; }
+              fy[a] = 2.0 * pc[a] - psij[a];
+              if (fy[a] < 0.0) { hv_y[a] = 0.0; neg++; }
+              fz[a] = 2.0 * pc[a] - psik[a];
+              if (fz[a] < 0.0) { hv_z[a] = 0.0; neg++; }
+            }
+            if (neg == old_neg) break;
+            old_neg = neg;
+            for (int a = 0; a < A; a++) {
+              pvx[a] = hv_x[a];
+              pvy[a] = hv_y[a];
+              pvz[a] = hv_z[a];
+              const double v = psi[a] + 0.5 * (psii[a] * g->mu[a] * g->hi * (1.0 + hv_x[a]) +
+                                                psij[a] * g->eta[a] * g->hj * (1.0 + hv_y[a]) +
+                                                psik[a] * g->xi[a] * g->hk * (1.0 + hv_z[a]));
+              const double den = (v <= 0.0) ? 0.0
+                  : (sig + g->mu[a] * g->hi * hv_x[a] + g->eta[a] * g->hj * hv_y[a] +
+                     g->xi[a] * g->hk * hv_z[a]);
+              rden[n * A + a] = den;
+              zero[a] = den < tolr;
+              pc[a] = zero[a] ? 0.0 : v / den;
+            }
+          }
+        }
+        for (int a = 0; a < A; a++) {
+          rpc[n * A + a] = pc[a];
+          rflag[n * A + a] = (unsigned char)((pvx[a] != 0.0) | ((pvy[a] != 0.0) << 1) |
+                                             ((pvz[a] != 0.0) << 2) | ((hv_x[a] != 0.0) << 3) |
+                                             ((hv_y[a] != 0.0) << 4) | ((hv_z[a] != 0.0) << 5) |
+                                             (zero[a] << 6));
+          psii[a] = (2.0 * pc[a] - psii[a]) * hv_x[a];
+          psij[a] = (2.0 * pc[a] - psij[a]) * hv_y[a];
+          psik[a] = (2.0 * pc[a] - psik[a]) * hv_z[a];
+        }
+        memcpy(ypencil + (size_t)xx * A, psij, sizeof(double) * A);
+        memcpy(zplane + ((size_t)yy * nx + xx) * A, psik, sizeof(double) * A);
+      }
+    }
+  }
+  /* reverse pass: adjoint faces, downstream cells first */
+  double *bx = psii, *by = psij, *bz = psik;   /* adjoint of the cell's outgoing faces */
+  for (int zz = nz - 1; zz >= 0; zz--) {
+    const int z = sz ? zz : nz - 1 - zz;
+    for (int yy = ny - 1; yy >= 0; yy--) {
+      const int y = sy ? yy : ny - 1 - yy;
+      for (int xx = nx - 1; xx >= 0; xx--) {
+        n--;
+        const int x = sx ? xx : nx - 1 - xx;
+        const size_t c = ((size_t)z * ny + y) * nx + x;
+        /* nothing downstream of the last cell along an axis */
+        if (xx == nx - 1) memset(bx, 0, sizeof(double) * A);
+        if (yy == ny - 1) memset(by, 0, sizeof(double) * A);
+        else memcpy(by, ypencil + (size_t)xx * A, sizeof(double) * A);
+        if (zz == nz - 1) memset(bz, 0, sizeof(double) * A);
+        else memcpy(bz, zplane + ((size_t)yy * nx + xx) * A, sizeof(double) * A);
+        const double *pb = phi_bar + (group * C + c) * cmom;
+        double *qb = qtot_bar + (group * C + c) * cmom;
+        double sb = 0.0;
+        for (int a = 0; a < A; a++) {
+          const unsigned f = rflag[n * A + a];
+          double pcb = pb[0] * g->w[a];
+          for (int k = 1; k < cmom; k++) pcb += ec[(size_t)k * A + a] * g->w[a] * pb[k];
+          const double hx = (f >> 3) & 1, hy = (f >> 4) & 1, hz = (f >> 5) & 1;
+          pcb += 2.0 * (hx * bx[a] + hy * by[a] + hz * bz[a]);
+          const double s = ((f >> 6) & 1) ? 0.0 : pcb / rden[n * A + a];
+          const double px = f & 1, py = (f >> 1) & 1, pz = (f >> 2) & 1;
+          /* adjoint of the incoming faces = adjoint of the upstream cells' outgoing faces */
+          bx[a] = -hx * bx[a] + s * 0.5 * (1.0 + px) * g->mu[a] * g->hi;
+          by[a] = -hy * by[a] + s * 0.5 * (1.0 + py) * g->eta[a] * g->hj;
+          bz[a] = -hz * bz[a] + s * 0.5 * (1.0 + pz) * g->xi[a] * g->hk;
+          qb[0] += s;
+          for (int k = 1; k < cmom; k++) qb[k] += ec[(size_t)k * A + a] * s;
+          sb -= s * rpc[n * A + a];
+        }
+        if (sigt_bar) sigt_bar[group * C + c] += sb;
+        /* bx carries to the upstream x neighbour; by, bz to the pencil/plane */
+        memcpy(ypencil + (size_t)xx * A, by, sizeof(double) * A);
+        memcpy(zplane + ((size_t)yy * nx + xx) * A, bz, sizeof(double) * A);
+      }
+    }
+  }
+  free(buf);
+  free(zero);
+  free(rflag);
+  free(rden);
+  free(rpc);
+}
+
+typedef struct {
+  const oracle_geom *g;
+  const double *qtot, *t_xs, *phi_bar;
+  double *qtot_bar, *sigt_bar;
+} adjoint_args;
+
+static void adjoint_group(void *arg, int grp) {
+  const adjoint_args *x = (const adjoint_args *)arg;
+  for (int corner = 0; corner < 8; corner++)
+    oracle_adjoint_octant_group(x->g, corner, grp, x->qtot, x->t_xs, x->phi_bar, x->qtot_bar,
+                                x->sigt_bar);
+}
+
+void oracle_adjoint_sweep(const oracle_geom *g, const double *qtot, const double *t_xs,
+                          const double *phi_bar, double *qtot_bar, double *sigt_bar) {
+  const size_t C = (size_t)g->nx * g->ny * g->nz;
+  memset(qtot_bar, 0, sizeof(double) * C * g->ng * g->cmom);
+  if (sigt_bar) memset(sigt_bar, 0, sizeof(double) * C * g->ng);
+  adjoint_args x = {g, qtot, t_xs, phi_bar, qtot_bar, sigt_bar};
+  par_for(g->ng, adjoint_group, &x);
+}
+
 /* inner.cc:283-324 and outer.cc:354-403 (scalar moment only) */
 int oracle_test_convergence(const oracle_geom *g, const double *flux,
                             const double *flux_prev, double epsi) {

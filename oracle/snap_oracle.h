@@ -74,6 +74,16 @@ void oracle_sweep_octant_group(const oracle_geom *g, int corner, int group,
  * octants still summed in octant order, so the result does not depend on n. */
 void oracle_sweep(const oracle_geom *g, const double *qtot, const double *t_xs,
                   double *flux);
+/* Adjoint of oracle_sweep with the fixup flags frozen at the forward state
+ * of qtot (no reference counterpart): qtot_bar [G][C][cmom] = transpose of
+ * the sweep applied to phi_bar [G][C][cmom], and (sigt_bar != NULL) the
+ * sensitivity to t_xs, sigt_bar [G][C].  Both are zeroed first. */
+void oracle_adjoint_octant_group(const oracle_geom *g, int corner, int group,
+                                 const double *qtot, const double *t_xs,
+                                 const double *phi_bar, double *qtot_bar,
+                                 double *sigt_bar);
+void oracle_adjoint_sweep(const oracle_geom *g, const double *qtot, const double *t_xs,
+                          const double *phi_bar, double *qtot_bar, double *sigt_bar);
 /* host threads used by oracle_sweep and oracle_outer_source (default 1) */
 void oracle_set_threads(int n);
 /* inner.cc:283-324 / outer.cc:354-403: returns 1 if converged */

@@ -151,3 +151,36 @@ def test_oracle_reproduces_deck4_fixture(golden_dir):
     assert np.array_equal(f[g["sample_g"], g["sample_c"], 0], g["sample_flux0"])
     assert np.array_equal(f[g["moment_g"], g["moment_c"], :], g["moment_flux"])
     assert rec["inners_per_outer"] == list(g["inners_per_outer"])
+
+
+@pytest.mark.parametrize("fixup,thick", [(False, False), (True, True)], ids=["plain", "fixups"])
+@pytest.mark.parametrize("nmom", [1, 2])
+def test_oracle_adjoint_sweep_is_transpose(fixup, thick, nmom):
+    """The CPU adjoint sweep (the check for the GPU adjoint) is the transpose
+    of the oracle's forward sweep at the same state: <phi_bar, sweep(q)> =
+    <adjoint(phi_bar), q> to rounding (the forward map is linear in q for
+    frozen fixup flags), and its t_xs sensitivity matches central
+    differences."""
+    d = P.Deck(6, 5, 4, nang=6, ng=2, nmom=nmom, fixup=fixup)
+    prob = P.make_problem(d)
+    if thick:
+        prob["sigt"] = prob["sigt"] * 40.0
+    o = Oracle(d)
+    t_xs, _ = o.expand(prob)
+    rng = np.random.default_rng(3)
+    q = rng.uniform(0.0, 1.0, size=(d.ng, d.cells, d.cmom))
+    if d.cmom > 1:
+        q[..., 1:] = rng.uniform(-0.3, 0.3, size=q[..., 1:].shape)
+    pb = rng.uniform(-1.0, 1.0, size=(d.ng, d.cells, d.cmom))
+    flux = o.sweep(q, t_xs)
+    qb, sb = o.adjoint_sweep(q, t_xs, pb)
+    lhs, rhs = float((pb * flux).sum()), float((qb * q).sum())
+    assert abs(lhs - rhs) <= 1e-13 * max(abs(lhs), 1.0)
+    # t_xs sensitivity at a few cells, central differences
+    for g, c in ((0, 7), (1, 33), (0, 101)):
+        h = 1e-6 * t_xs[g, c]
+        tp, tm = t_xs.copy(), t_xs.copy()
+        tp[g, c] += h
+        tm[g, c] -= h
+        fd = (float((pb * o.sweep(q, tp)).sum()) - float((pb * o.sweep(q, tm)).sum())) / (2 * h)
+        assert abs(sb[g, c] - fd) <= 1e-6 * max(abs(fd), 1e-6), (g, c, sb[g, c], fd)
