@@ -376,16 +376,17 @@ def test_fp32_tf32_solve_error(tf32_sweep):
                                P.Deck(16, 16, 8, nang=4, ng=33, nmom=3),
                                P.Deck(16, 16, 8, nang=4, ng=32, nmom=4),
                                P.Deck(16, 8, 8, nang=4, ng=64, nmom=3),
-                               P.Deck(7, 5, 3, nang=4, ng=32, nmom=4)],
+                               P.Deck(7, 5, 3, nang=4, ng=32, nmom=4),
+                               P.Deck(7, 5, 3, nang=4, ng=20, nmom=3)],
                          ids=["G20_cmom16", "G4_cmom1", "G33_cmom9", "G32_cmom16", "G64_cmom9",
-                              "ragged_cells"])
+                              "ragged_cells", "unaligned_runs"])
 def test_outer_source_tc_matches_fp64(d):
     """The split-BF16 tensor-core outer source (tcgen05.mma, accumulators in
     tensor memory) against the FP64 one (itself at 1e-12 of the oracle): the
     scattering term within 1e-4 of its largest magnitude per moment, the
-    fixed source exact, on 128-cell tiles that mix the two materials, group
-    counts that are not multiples of 16 and a last tile that is mostly
-    empty."""
+    fixed source exact, on batches that mix the two materials, group counts
+    that are not multiples of 16, a last batch that is mostly empty, and
+    per-group runs that are not 16-byte aligned (no bulk-copy stages)."""
     snap = snap_ctx(d)
     dp = snap.device_problem(P.make_problem(d))
     flux = dev(random_qtot(d, 5))
