@@ -11,6 +11,21 @@
 
 namespace snapb200 {
 
+// Order of the forward sweep's MMA operand tables (per octant; lane l of the
+// m8n8k4 fragment).  Paired order (the FP64 sweep): for the source
+// expansion, k-tile kt of angle tile nt, with an even k-tile count k-tiles
+// 2i and 2i+1 of one angle tile are adjacent, so one 16-byte shared-memory
+// load feeds two MMAs; for the moment accumulation, angle slot t and moment
+// tile mt, the moment tiles of one slot are adjacent.  Otherwise (the FP32
+// sweep, whose register budget keeps single loads) lane-minor.
+__host__ __device__ inline int b1_slot(int kt, int nt, int l, int NT, int MK, bool paired) {
+  return paired && MK % 2 == 0 ? (((kt >> 1) * NT + nt) * 32 + l) * 2 + (kt & 1)
+                               : (kt * NT + nt) * 32 + l;
+}
+__host__ __device__ inline int b2_slot(int t, int mt, int l, int MN, bool paired) {
+  return paired ? (t * 32 + l) * MN + mt : (t * MN + mt) * 32 + l;
+}
+
 // Parameters of one launch of the persistent sweep kernel.
 struct SweepParams {
   int nx, ny, nz;

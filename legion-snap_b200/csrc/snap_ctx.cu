@@ -192,7 +192,8 @@ void build_tables(const snap_ctx *c, std::vector<T> &coef, std::vector<double> &
       for (int nt = 0; nt < NT; ++nt)
         for (int l = 0; l < 32; ++l) {
           const int m = (l & 3) * MK + kt, a = 8 * nt + (l >> 2);
-          bt1[(size_t)o * B1 + (kt * NT + nt) * 32 + l] = (m < M && a < A) ? ec(o, m, a) : 0.0;
+          bt1[(size_t)o * B1 + b1_slot(kt, nt, l, NT, MK, sizeof(T) == 8)] =
+              (m < M && a < A) ? ec(o, m, a) : 0.0;
         }
     for (int t = 0; t < 2 * NT; ++t)
       for (int mt = 0; mt < MN; ++mt)
@@ -201,7 +202,7 @@ void build_tables(const snap_ctx *c, std::vector<T> &coef, std::vector<double> &
           const int a = 8 * nt + 2 * (l & 3) + h;
           const int r = l >> 2;
           const int m = (r >> 1) * 2 * MN + 2 * mt + (r & 1);
-          bt2[(size_t)o * B2 + (t * MN + mt) * 32 + l] =
+          bt2[(size_t)o * B2 + b2_slot(t, mt, l, MN, sizeof(T) == 8)] =
               (m < M && a < A) ? ec(o, m, a) * c->w[a] : 0.0;
         }
   }

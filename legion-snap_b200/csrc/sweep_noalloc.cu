@@ -83,14 +83,16 @@ __global__ void noalloc_tables_kernel(const double *mu, const double *eta, const
       const int j = i - 4 * AP, o = j / B1, rem = j % B1;
       const int kt = rem / (NT * 32), nt = (rem / 32) % NT, l = rem % 32;
       const int m = (l & 3) * MK + kt, a = 8 * nt + (l >> 2);
-      bt1[j] = (m < M && a < A) ? ec[((size_t)o * M + m) * A + a] : 0.0;
+      bt1[(size_t)o * B1 + b1_slot(kt, nt, l, NT, MK, true)] =
+          (m < M && a < A) ? ec[((size_t)o * M + m) * A + a] : 0.0;
     } else {
       const int j = i - 4 * AP - 8 * B1, o = j / B2, rem = j % B2;
       const int t = rem / (MN * 32), mt = (rem / 32) % MN, l = rem % 32;
       const int a = 8 * (t >> 1) + 2 * (l & 3) + (t & 1);
       const int r = l >> 2;
       const int m = (r >> 1) * 2 * MN + 2 * mt + (r & 1);
-      bt2[j] = (m < M && a < A) ? ec[((size_t)o * M + m) * A + a] * w[a] : 0.0;
+      bt2[(size_t)o * B2 + b2_slot(t, mt, l, MN, true)] =
+          (m < M && a < A) ? ec[((size_t)o * M + m) * A + a] * w[a] : 0.0;
     }
   }
 }
