@@ -102,6 +102,9 @@ SWEEP_DECKS = [
     P.Deck(16, 8, 24, nang=24, ng=2, nmom=2),            # adjoint-deck shape, 4 moments
     P.Deck(8, 16, 8, nang=48, ng=2, nmom=3),             # deck-3/5 angles, 9 moments
     P.Deck(8, 8, 5, nang=3, ng=1, nmom=1),               # tiny: one tile, ragged angle tile
+    P.Deck(8, 8, 8, nang=32, ng=2, nmom=4),              # 4 angle tiles, 16 moments
+    P.Deck(8, 8, 6, nang=56, ng=1, nmom=2),              # 7 angle tiles
+    P.Deck(8, 4, 6, nang=64, ng=2, nmom=3),              # 8 angle tiles (the tiled kernel's widest)
 ]
 
 
@@ -146,11 +149,13 @@ def thick_point_source(d):
     return prob
 
 
-@pytest.mark.parametrize("nmom", [1, 2])
-def test_sweep_fixup_heavy(nmom):
+@pytest.mark.parametrize("nang,nmom", [(10, 1), (10, 2), (36, 4), (64, 2)],
+                         ids=["A10_M1", "A10_M4", "A36_M16", "A64_M4"])
+def test_sweep_fixup_heavy(nang, nmom):
     """Optically thick cells around a point source: most cells take the
-    negative-flux fixup path."""
-    d = P.Deck(16, 16, 8, nang=10, ng=2, nmom=nmom)
+    negative-flux fixup path (36 angles: the 3-CTA shape whose fixup works on
+    faces and fluxes parked in shared memory; 64: the widest tile)."""
+    d = P.Deck(16, 16, 8, nang=nang, ng=2, nmom=nmom)
     prob = thick_point_source(d)
     o = Oracle(d)
     t_xs, s_xs = o.expand(prob)
@@ -312,8 +317,9 @@ def test_fp32_sweep_error(d):
     assert moment_err(got, ref) < FP32_TOL
 
 
-def test_fp32_sweep_fixup_heavy():
-    d = P.Deck(16, 16, 8, nang=10, ng=2, nmom=2)
+@pytest.mark.parametrize("nang", [10, 36])
+def test_fp32_sweep_fixup_heavy(nang):
+    d = P.Deck(16, 16, 8, nang=nang, ng=2, nmom=2)
     prob = thick_point_source(d)
     o = Oracle(d)
     t_xs, s_xs = o.expand(prob)
