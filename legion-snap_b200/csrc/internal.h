@@ -39,8 +39,9 @@ struct SweepParams {
   int atomic_flux; // phi_slots is the FP64 flux [G][C][M]: every octant adds into it atomically
   int fixup;
   int withhold_item1;     // fault injection: work item + 1 whose warps never publish progress (0: none)
+  int gchain = 1;  // groups per work item, walked as one chained z column (sweep kernel)
   long long timeout_ns;
-  const int *item_table;  // item -> (sweep << 16) | (tx << 8) | ty
+  const int *item_table;  // item -> (sweep << 16) | (tx << 8) | ty; sweep = octant * chains + chain
   const int *item_index;  // [sweep][tx][ty] -> item
   const void *qtot;       // [G][C][M]
   const void *t_xs;       // [G][C]

@@ -62,6 +62,11 @@ struct snap_ctx {
   void *d_sbar_slots = nullptr;                 // adjoint of t_xs per octant slot
   bool state_recorded = false;
   int *d_item_table = nullptr, *d_item_index = nullptr;
+  // the inner iteration's sweep: work items of gchain groups each (their z
+  // columns walked as one), so a warp's pipeline fills and drains once per
+  // chain instead of once per group
+  int gchain = 1, n_chain_items = 0, grid_chain = 0;
+  int *d_chain_table = nullptr, *d_chain_index = nullptr;
   // FP32 contexts: the split-TF32 tensor-core sweep over group pairs
   int tc32 = 0;
   int n_pair_items = 0, grid_tc = 0;
@@ -133,6 +138,8 @@ void free_ctx(snap_ctx *c) {
   cudaFree(c->d_sbar_slots);
   cudaFree(c->d_item_table);
   cudaFree(c->d_item_index);
+  cudaFree(c->d_chain_table);
+  cudaFree(c->d_chain_index);
   cudaFree(c->d_pair_table);
   cudaFree(c->d_pair_index);
   cudaFree(c->d_tc1);
@@ -396,6 +403,13 @@ int sweep_launches(snap_ctx *c, const void *qtot, const void *t_xs, cudaStream_t
     grid = c->grid_td;
   }
   const bool tc = c->tc32 && mode != 2;
+  if (c->gchain > 1 && mode == 0 && atomic_flux && !td && !batch && !tc) {
+    p.gchain = c->gchain;
+    p.n_items = c->n_chain_items;
+    p.item_table = c->d_chain_table;
+    p.item_index = c->d_chain_index;
+    grid = c->grid_chain;
+  }
   if (tc) {
     p.n_items = c->n_pair_items;
     p.item_table = c->d_pair_table;
@@ -797,6 +811,30 @@ int snap_create(const snap_config *cfg, int device, snap_ctx **out) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   c->grid = std::min(blocks * sms, c->n_items);
   if (const char *ge = getenv("SNAP_B200_GRID")) c->grid = std::max(1, std::min(atoi(ge), c->grid));
+  // group chains: the largest divisor of G that still leaves 16 work items
+  // per resident CTA (load balance over the queue); SNAP_B200_GROUP_CHAIN
+  // sets it (a divisor of G; 1: none).  A divisor keeps every item's face
+  // buffers inside the ones allocated above.
+  {
+    int gc = 0;
+    if (const char *ce = getenv("SNAP_B200_GROUP_CHAIN")) gc = atoi(ce);
+    if (gc < 1 || gc > G || G % gc != 0) {
+      gc = 1;
+      for (int d = 2; d <= G; ++d)
+        if (G % d == 0 && (long long)c->n_items / d >= 16LL * c->grid) gc = d;
+    }
+    if (gc > 1 && !c->wide_only && !c->tc32) {
+      build_items(P, G / gc, c->tiles_x, c->tiles_y, table, index);
+      if ((rc = upload((void **)&c->d_chain_table, table)) ||
+          (rc = upload((void **)&c->d_chain_index, index))) {
+        free_ctx(c);
+        return rc;
+      }
+      c->gchain = gc;
+      c->n_chain_items = (int)table.size();
+      c->grid_chain = std::min(c->grid, c->n_chain_items);
+    }
+  }
   if (c->tc32) {
     e = sweep_tc32_occupancy(c->shape, &blocks, &smem);
     if (e != cudaSuccess || blocks < 1) {

@@ -233,6 +233,46 @@ def test_solve_multimoment_matches_oracle():
     assert rec["inners_per_outer"] == rref["inners_per_outer"]
 
 
+@pytest.mark.parametrize("env", [dict(SNAP_B200_GROUP_CHAIN="2"), dict(SNAP_B200_GROUP_CHAIN="3"),
+                                 dict(SNAP_B200_GROUP_CHAIN="6"),
+                                 dict(SNAP_B200_GROUP_CHAIN="3", SNAP_B200_GRID="1"),
+                                 dict(SNAP_B200_GROUP_CHAIN="2", SNAP_B200_OCTANTS_PER_LAUNCH="2")],
+                         ids=["chain2", "chain3", "chain6", "chain3_grid1", "chain2_P2"])
+def test_solve_group_chains_match_oracle(env, monkeypatch):
+    """The inner iteration's sweep with work items of several groups (their z
+    columns walked as one chained column; the z face restarts at the vacuum
+    boundary of each group): the same solve as the oracle, also with one CTA
+    walking every item and with fewer octants per launch."""
+    for k, v in env.items():
+        monkeypatch.setenv(k, v)
+    d = P.Deck(16, 16, 8, nang=12, ng=6, nmom=2, epsi=1e-6, iitm=3, oitm=4)
+    prob = P.make_problem(d)
+    ref, rref = Oracle(d).solve(prob)
+    snap = snap_ctx(d)
+    flux, rec = snap.transport_solve(snap.device_problem(prob))
+    got = flux.cpu().numpy()
+    assert rel_err(got[..., 0], ref[..., 0]) < TOL
+    assert moment_err(got, ref) < TOL
+    assert rec["inners_per_outer"] == rref["inners_per_outer"]
+
+
+def test_fp32_solve_group_chains(monkeypatch):
+    """FP32 sweep with chained groups: within the FP32 tolerance of the FP64
+    oracle, and equal to the unchained FP32 solve up to the atomic order of
+    the octant sums."""
+    d = P.Deck(16, 16, 8, nang=12, ng=6, nmom=2, epsi=1e-6, iitm=3, oitm=4)
+    prob = P.make_problem(d)
+    ref, _ = Oracle(d).solve(prob)
+    out = []
+    for gc in ("1", "3"):
+        monkeypatch.setenv("SNAP_B200_GROUP_CHAIN", gc)
+        snap = snap_ctx32(d)
+        flux, _ = snap.transport_solve(snap.device_problem(prob))
+        out.append(flux.cpu().numpy())
+    assert rel_err(out[1][..., 0], ref[..., 0]) < FP32_TOL
+    assert rel_err(out[1][..., 0], out[0][..., 0]) < 1e-5
+
+
 def check_oracle_fixture(g, flux, rec, tol):
     """A converged solve against an oracle fixture (tests/golden/*_oracle.npz):
     the scalar flux at the seeded samples, per-group sums and maxima (relative,
