@@ -811,17 +811,27 @@ int snap_create(const snap_config *cfg, int device, snap_ctx **out) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   c->grid = std::min(blocks * sms, c->n_items);
   if (const char *ge = getenv("SNAP_B200_GRID")) c->grid = std::max(1, std::min(atoi(ge), c->grid));
-  // group chains: the largest divisor of G that still leaves 16 work items
-  // per resident CTA (load balance over the queue); SNAP_B200_GROUP_CHAIN
-  // sets it (a divisor of G; 1: none).  A divisor keeps every item's face
-  // buffers inside the ones allocated above.
+  // group chains: the smallest divisor of G whose chained column has at
+  // least 1024 planes (the pipeline's fill and drain then cost under 1 %), or
+  // a shorter one where that would leave fewer than 12 work items per
+  // resident CTA (load balance over the queue).  Deck 2 (64 planes, 32
+  // groups, FP64 sweep ms): chains of 1 / 2 / 4 / 8 / 16 groups 18.8 / 17.8 /
+  // 17.4 / 17.7 / 18.7; FP32 with 2 / 4 / 8: 12.33 / 12.20 / 12.60; 128^3 /
+  // 64 groups (FP64, from a zero flux): 1 / 2 / 8 / 32: 362 / 350 / 346 / 365.
+  // SNAP_B200_GROUP_CHAIN sets it (a divisor of G; 1: none).  A divisor
+  // keeps every item's face buffers inside the ones allocated above.
   {
     int gc = 0;
     if (const char *ce = getenv("SNAP_B200_GROUP_CHAIN")) gc = atoi(ce);
     if (gc < 1 || gc > G || G % gc != 0) {
-      gc = 1;
-      for (int d = 2; d <= G; ++d)
-        if (G % d == 0 && (long long)c->n_items / d >= 16LL * c->grid) gc = d;
+      gc = G;
+      for (int d = G; d >= 1; --d)
+        if (G % d == 0 && (long long)d * cfg->nz >= 1024) gc = d;
+      while (gc > 1 && (long long)c->n_items / gc < 12LL * c->grid) {
+        int d = gc - 1;
+        while (G % d != 0) --d;
+        gc = d;
+      }
     }
     if (gc > 1 && !c->wide_only && !c->tc32) {
       build_items(P, G / gc, c->tiles_x, c->tiles_y, table, index);
