@@ -70,7 +70,9 @@ typedef struct snap_ctx snap_ctx;
  * per octant and group; up to 128 angles the cells of a diagonal plane in
  * flight, one warp per cell, else cell by cell up to 2048 angles; FP64
  * contexts only; no adjoint).  SNAP_B200_WAVE=0 selects the cell-by-cell
- * form always.
+ * form always.  The tiled kernel's inner-iteration sweeps walk several
+ * groups' z columns per work item (a chain of groups, sized at creation);
+ * SNAP_B200_GROUP_CHAIN=n sets the chain length (a divisor of ng; 1: none).
  * Replaces InitGPUSweep -> initialize_gpu_context (init.cc:215-236,
  * gpu_sweep.cu:71-273). */
 int snap_create(const snap_config *cfg, int device, snap_ctx **out);
