@@ -48,10 +48,14 @@ struct Shape {
   static constexpr int YST = 2 * 8 * AP;
   static constexpr size_t SMEM_BYTES =
       sizeof(double) * (B1 + B2) + sizeof(T) * (4 * AP + YRING + XST + YST);
+  // CTAs per SM the register budget is sized for: 3 (168 registers; no
+  // spills in FP32, at most a few bytes in FP64 up to 5 angle tiles), 1 for
+  // FP64 from 6 angle tiles up, where 168 registers would spill
+  static constexpr int MIN_BLOCKS = TY == 8 || (sizeof(T) == 8 && NT >= 6) ? 1 : 3;
 };
 
 template <typename T, int NT, int MK, int TY>
-__global__ void __launch_bounds__(TY * 32, 1) adjoint_kernel(const SweepParams p) {
+__global__ void __launch_bounds__(TY * 32, (Shape<T, NT, MK, TY>::MIN_BLOCKS)) adjoint_kernel(const SweepParams p) {
   using S = Shape<T, NT, MK, TY>;
   using T2 = typename Vec2<T>::type;
   constexpr int AP = S::AP, S2 = S::S2, MN = S::MN;
