@@ -7,6 +7,7 @@ name can capture a launch of it on a few GB of device memory:
     python -m snap_b200.cases sweep --deck 2 --groups 4 [--precision fp32] [--iters 3]
     python -m snap_b200.cases outer-source --deck 2 [--form tcgen05] [--calls 3]
     python -m snap_b200.cases input-deck tests/decks/tiny_4K_1x1x1.in [--inners 3] [--general]
+    python -m snap_b200.cases adjoint [--deck 4]
 
 sweep: inner iterations (inner source, sweep of every octant and group,
 inner test) of a benchmark deck with its group count overridden, from a
@@ -14,7 +15,9 @@ zero flux and the deck's fixed source.  outer-source: the group-to-group
 outer source of a benchmark deck from a seeded random flux, in the FP64
 tensor-core form or the split-BF16 tcgen05 form.  input-deck: one time step
 of a reference input deck, capped at one outer and `--inners` inner
-iterations (`--general` pins the general sweep kernel).
+iterations (`--general` pins the general sweep kernel).  adjoint: a
+converged forward solve of a benchmark deck, then the adjoint solve of a
+detector response on the 4x4x4 far corner (weights 1/g).
 """
 from __future__ import annotations
 
@@ -80,6 +83,24 @@ def input_deck_case(path: str, inners: int, general: bool) -> None:
     snap.close()
 
 
+def adjoint_case(deck: int) -> None:
+    d = P.deck(deck)
+    snap = Snap(d)
+    dp = snap.device_problem(P.make_problem(d))
+    r = torch.zeros(d.ng, d.nz, d.ny, d.nx, dtype=torch.float64, device="cuda")
+    r[:, -4:, -4:, -4:] = (1.0 / torch.arange(1, d.ng + 1, dtype=torch.float64,
+                                              device="cuda"))[:, None, None, None]
+    r = r.reshape(d.ng, d.cells)
+    (flux, rec), ms = _timed(lambda: snap.transport_solve(dp))
+    print(f"forward solve: {rec['inner_total']} inner iterations, {ms:.3f} ms")
+    t_xs = snap.expand_cross_section(dp["sigt"], dp["mat"])
+    if "sigt_scale" in dp:   # the per-cell sigma_t perturbation of the adjoint deck
+        t_xs = t_xs * dp["sigt_scale"][None, :]
+    g, ms = _timed(lambda: snap.adjoint_solve(dp, t_xs, flux, r))
+    print(f"adjoint solve: {g['iterations']} iterations, {ms:.3f} ms")
+    snap.close()
+
+
 def main(argv=None) -> None:
     ap = argparse.ArgumentParser(prog="python -m snap_b200.cases")
     sub = ap.add_subparsers(dest="case", required=True)
@@ -96,13 +117,17 @@ def main(argv=None) -> None:
     i.add_argument("path")
     i.add_argument("--inners", type=int, default=3)
     i.add_argument("--general", action="store_true")
+    j = sub.add_parser("adjoint")
+    j.add_argument("--deck", type=int, default=4)
     a = ap.parse_args(argv)
     if a.case == "sweep":
         sweep_case(a.deck, a.groups, a.precision, a.iters)
     elif a.case == "outer-source":
         outer_source_case(a.deck, a.form, a.calls)
-    else:
+    elif a.case == "input-deck":
         input_deck_case(a.path, a.inners, a.general)
+    else:
+        adjoint_case(a.deck)
 
 
 if __name__ == "__main__":
