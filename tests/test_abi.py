@@ -75,3 +75,21 @@ def test_create_rejects_null_arguments():
     assert abi.STATUS.get(lib.snap_create(None, 0, ctypes.byref(h))) == "SNAP_ERR_BAD_ARG"
     assert abi.STATUS.get(lib.snap_create(None, 0, None)) == "SNAP_ERR_BAD_ARG"
     assert lib.snap_destroy(None) in (0, 1)   # destroying nothing is harmless
+
+
+def test_profiling_cases_cli(monkeypatch):
+    """The single-kernel profiling cases the profile summaries name parse
+    their documented command lines (no GPU call: parsing only)."""
+    monkeypatch.syspath_prepend(str(ROOT / "legion-snap_b200"))
+    from snap_b200 import cases
+    called = {}
+    for name in ("sweep_case", "outer_source_case", "input_deck_case", "adjoint_case"):
+        monkeypatch.setattr(cases, name, lambda *a, _n=name: called.setdefault(_n, a))
+    cases.main(["sweep", "--deck", "2", "--groups", "4", "--precision", "fp32"])
+    cases.main(["outer-source", "--deck", "2", "--form", "tcgen05", "--calls", "3"])
+    cases.main(["input-deck", "tests/decks/tiny_4K_1x1x1.in", "--inners", "3"])
+    cases.main(["adjoint", "--deck", "4"])
+    assert called["sweep_case"] == (2, 4, "fp32", 3)
+    assert called["outer_source_case"] == (2, "tcgen05", 3)
+    assert called["input_deck_case"] == ("tests/decks/tiny_4K_1x1x1.in", 3, False)
+    assert called["adjoint_case"] == (4,)
