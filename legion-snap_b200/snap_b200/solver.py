@@ -289,15 +289,17 @@ def _records(info) -> list:
             for r in info.records[:info.records_len]]
 
 
-def fp64_finish(deck: Deck, dprob: dict, flux: torch.Tensor, outers: int = 1, device: int = 0):
+def fp64_finish(deck: Deck, dprob: dict, flux: torch.Tensor, outers: int = 1, device: int = 0,
+                max_inners: int | None = None):
     """FP64 refinement of a mixed-precision solution: `outers` outer
     iterations of the FP64 path (FP64 outer source, FP64 sweeps until the
-    inner test passes or iitm) started from `flux` (the converged FP32-form
-    flux moments, float64), through the task-level C ABI of an FP64 context.
-    The outer iteration contracts the FP32 rounding error like any other
-    error, so one outer removes most of it.  The FP32 context should be
-    destroyed first when memory is tight.  Returns the refined flux (a new
-    tensor) and the device time and iteration counts."""
+    inner test passes, iitm or `max_inners`) started from `flux` (the
+    converged FP32-form flux moments, float64), through the task-level C ABI
+    of an FP64 context.  Each FP64 iteration contracts the FP32 rounding
+    error like any other error, so one outer removes most of it and a single
+    sweep a large part.  The FP32 context should be destroyed first when
+    memory is tight.  Returns the refined flux (a new tensor) and the device
+    time and iteration counts."""
     snap = Snap(deck, precision="fp64", device=device)
     try:
         flux = flux.clone()
@@ -312,7 +314,7 @@ def fp64_finish(deck: Deck, dprob: dict, flux: torch.Tensor, outers: int = 1, de
         inners = 0
         for _ in range(outers):
             q2 = snap.calc_outer_source(dprob["qi"], dprob["slgg"], dprob["mat"], flux)
-            for _ in range(deck.iitm):
+            for _ in range(deck.iitm if max_inners is None else min(deck.iitm, max_inners)):
                 inners += 1
                 if snap.inner_iteration(s_xs, q2, t_xs, flux, qtot):
                     break
