@@ -37,11 +37,16 @@ constexpr unsigned FULL = 0xffffffffu;
 constexpr int MAX_THREADS = 512;
 constexpr int MAX_WARPS = MAX_THREADS / 32;
 
-// MAXT: the CTA size the register budget is sized for (128 threads leave
-// room for four angles per thread without spilling).
+// MAXT: the CTA size the register budget is sized for: 128 registers per
+// thread at any size, so that 4 CTAs of 128 threads (or 2 of 256) are
+// resident per SM.  A sweep is one walk over the cells per wave of resident
+// CTAs (one CTA per octant and group), so the register footprint per angle
+// sets the number of waves: the per-angle constants live in shared memory,
+// the fixup flags in bit masks, and the angular source is recomputed in the
+// rare fixup passes instead of being kept.
 template <int APT, int MAXT>
-__global__ void __launch_bounds__(MAXT) wide_sweep_kernel(const WideParams p) {
-  extern __shared__ double s_red[];   // [warps][nx][M] per-warp moment partials of a pencil
+__global__ void __launch_bounds__(MAXT, (MAXT >= 512 ? 1 : 512 / MAXT)) wide_sweep_kernel(const WideParams p) {
+  extern __shared__ double s_dyn[];
   __shared__ int s_cnt[MAX_WARPS];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nwarps = blockDim.x >> 5;
@@ -59,32 +64,30 @@ __global__ void __launch_bounds__(MAXT) wide_sweep_kernel(const WideParams p) {
   double *ypen = p.ypen + (size_t)blockIdx.x * nx * A;
   double *zpl = p.zpl + (size_t)blockIdx.x * nx * ny * A;
   const double *ec = p.ec + (size_t)o * M * A;
-
-  // this thread's angles and their constants
-  int ang[APT];
-  bool on[APT];
-  double cx[APT], cy[APT], cz[APT], wt[APT];
+  double *s_red = s_dyn;                                   // [warps][nx][M] per-warp moment partials
+  double *s_cx = s_red + (size_t)nwarps * nx * M;          // [A] hi*mu, then hj*eta, hk*xi, w
+  double *s_cy = s_cx + A, *s_cz = s_cy + A, *s_w = s_cz + A;
+  for (int a = tid; a < A; a += blockDim.x) {
+    s_cx[a] = p.mu[a] * p.hi;
+    s_cy[a] = p.eta[a] * p.hj;
+    s_cz[a] = p.xi[a] * p.hk;
+    s_w[a] = p.w[a];
+  }
+  __syncthreads();
+  // this thread's angles: tid + k * blockDim.x
+  auto angle = [&](int k) { return tid + k * (int)blockDim.x; };
   double xin[APT];   // x face carried along the pencil
 #pragma unroll
-  for (int k = 0; k < APT; ++k) {
-    ang[k] = tid + k * blockDim.x;
-    on[k] = ang[k] < A;
-    const int a = on[k] ? ang[k] : 0;
-    cx[k] = p.mu[a] * p.hi;
-    cy[k] = p.eta[a] * p.hj;
-    cz[k] = p.xi[a] * p.hk;
-    wt[k] = on[k] ? p.w[a] : 0.0;
-    xin[k] = 0.0;
-  }
+  for (int k = 0; k < APT; ++k) xin[k] = 0.0;
 
-  // The inputs of a cell (sigma_t, the scalar source, and per angle the MMS
-  // source, the time-edge flux and the incoming y and z faces) are loaded one
-  // cell ahead, while the cell before is computed.  The faces a cell reads
-  // were written by this thread at an earlier cell, except when the mesh is
-  // one cell wide (nx = 1: the y face of the next pencil is this cell's; nx
-  // = ny = 1: so is the z face), where they are forwarded from registers.
+  // The inputs of a cell (sigma_t, the scalar source, and per angle the
+  // time-edge flux and the incoming y and z faces) are loaded one cell
+  // ahead, while the cell before is computed.  The faces a cell reads were
+  // written by this thread at an earlier cell, except when the mesh is one
+  // cell wide (nx = 1: the y face of the next pencil is this cell's; nx =
+  // ny = 1: so is the z face), where they are forwarded from registers.
   double n_sig = 0.0, n_q0 = 0.0;
-  double n_qim[APT], n_iy[APT], n_iz[APT], n_it[APT];
+  double n_iy[APT], n_iz[APT], n_it[APT];
   auto load_cell = [&](int xx, int yy, int zz) {
     const int x = sx ? xx : nx - 1 - xx, y = sy ? yy : ny - 1 - yy, z = sz ? zz : nz - 1 - zz;
     const long long c = ((long long)z * ny + y) * nx + x;
@@ -92,11 +95,11 @@ __global__ void __launch_bounds__(MAXT) wide_sweep_kernel(const WideParams p) {
     n_q0 = __ldg(qg + c * M);
 #pragma unroll
     for (int k = 0; k < APT; ++k) {
-      const int a = on[k] ? ang[k] : 0;
-      n_qim[k] = (p.qim && on[k]) ? p.qim[(field + c) * A + a] : 0.0;
-      n_it[k] = (tt && on[k]) ? p.tf_in[(field + c) * A + a] : 0.0;
-      n_iy[k] = (yy == 0 || !on[k]) ? 0.0 : ypen[(size_t)xx * A + a];
-      n_iz[k] = (zz == 0 || !on[k]) ? 0.0 : zpl[((size_t)yy * nx + xx) * A + a];
+      const int a = angle(k);
+      const bool on = a < A;
+      n_it[k] = (tt && on) ? p.tf_in[(field + c) * A + a] : 0.0;
+      n_iy[k] = (yy == 0 || !on) ? 0.0 : ypen[(size_t)xx * A + a];
+      n_iz[k] = (zz == 0 || !on) ? 0.0 : zpl[((size_t)yy * nx + xx) * A + a];
     }
   };
   load_cell(0, 0, 0);
@@ -111,13 +114,12 @@ __global__ void __launch_bounds__(MAXT) wide_sweep_kernel(const WideParams p) {
         const double *q = qg + c * M;
         const double sig = n_sig;
         const double q0 = n_q0;
-        double pc[APT], psi[APT], iy[APT], iz[APT], it[APT], qm[APT];
+        double pc[APT], iy[APT], iz[APT], it[APT];
 #pragma unroll
         for (int k = 0; k < APT; ++k) {
           iy[k] = n_iy[k];
           iz[k] = n_iz[k];
           it[k] = n_it[k];
-          qm[k] = n_qim[k];
         }
         // the next cell's inputs
         const bool more = xx + 1 < nx || yy + 1 < ny || zz + 1 < nz;
@@ -125,47 +127,56 @@ __global__ void __launch_bounds__(MAXT) wide_sweep_kernel(const WideParams p) {
         const int nyy = xx + 1 < nx ? yy : (yy + 1 < ny ? yy + 1 : 0);
         const int nzz = (xx + 1 < nx || yy + 1 < ny) ? zz : zz + 1;
         if (more) load_cell(nxx, nyy, nzz);
+        // angular source of angle k (sweep.cc:354-375); the same operations
+        // in the same order wherever it is needed
+        auto source = [&](int k) {
+          const int a = angle(k);
+          double s = q0;
+          for (int m = 1; m < M; ++m) s += ec[(size_t)m * A + a] * __ldg(q + m);
+          if (p.qim) s += p.qim[(field + c) * A + a];
+          return s;
+        };
+        if (xx == 0) {
+#pragma unroll
+          for (int k = 0; k < APT; ++k) xin[k] = 0.0;   // vacuum x boundary (single chunk)
+        }
         bool neg = false;
 #pragma unroll
         for (int k = 0; k < APT; ++k) {
-          const int a = on[k] ? ang[k] : 0;
-          // angular source (sweep.cc:354-375)
-          double s = q0;
-          for (int m = 1; m < M; ++m) s += ec[(size_t)m * A + a] * __ldg(q + m);
-          if (p.qim && on[k]) s += qm[k];
-          psi[k] = s;
-          if (xx == 0) xin[k] = 0.0;   // vacuum x boundary (single chunk)
+          const int a = angle(k);
+          const bool on = a < A;
+          const int ak = on ? a : 0;
+          const double cx = s_cx[ak], cy = s_cy[ak], cz = s_cz[ak];
           // diamond difference with the geometry parameter (expxs.cc:384-385,
           // sweep.cc:377-423)
-          double v = s + xin[k] * cx[k];
-          v += iy[k] * cy[k];
-          v += iz[k] * cz[k];
+          double v = (on ? source(k) : 0.0) + xin[k] * cx;
+          v += iy[k] * cy;
+          v += iz[k] * cz;
           if (tt) v += vd * it[k];
-          const double dinv = __drcp_rn(sig + vd + cx[k] + cy[k] + cz[k]);
-          v = on[k] ? v * dinv : 0.0;
+          const double dinv = __drcp_rn(sig + vd + cx + cy + cz);
+          v = on ? v * dinv : 0.0;
           pc[k] = v;
           const double v2 = 2.0 * v;
           neg = neg || (v2 - xin[k] < 0.0) || (v2 - iy[k] < 0.0) || (v2 - iz[k] < 0.0) ||
                 (tt && v2 - it[k] < 0.0);
         }
-        // negative-flux fixup (sweep.cc:425-533): flags per angle and face,
-        // the count of negative faces summed over every angle of the cell,
-        // every angle recomputed until the count stops changing
-        double hx[APT], hy[APT], hz[APT], ht[APT];
-#pragma unroll
-        for (int k = 0; k < APT; ++k) hx[k] = hy[k] = hz[k] = ht[k] = 1.0;
+        // negative-flux fixup (sweep.cc:425-533): flags per angle and face
+        // (bit k of each mask: 1 = the face keeps its value), the count of
+        // negative faces summed over every angle of the cell, every angle
+        // recomputed until the count stops changing
+        unsigned hxm = ~0u, hym = ~0u, hzm = ~0u, htm = ~0u;
         if (p.fixup && __syncthreads_or(neg)) {
           int old = 0;
           for (int iter = 0; iter < 4 * 2048 + 4; ++iter) {
             int cnt = 0;
 #pragma unroll
             for (int k = 0; k < APT; ++k) {
-              if (!on[k]) continue;
+              if (angle(k) >= A) continue;
               const double v2 = 2.0 * pc[k];
-              if (v2 - xin[k] < 0.0) { hx[k] = 0.0; ++cnt; }
-              if (v2 - iy[k] < 0.0) { hy[k] = 0.0; ++cnt; }
-              if (v2 - iz[k] < 0.0) { hz[k] = 0.0; ++cnt; }
-              if (tt && v2 - it[k] < 0.0) { ht[k] = 0.0; ++cnt; }
+              if (v2 - xin[k] < 0.0) { hxm &= ~(1u << k); ++cnt; }
+              if (v2 - iy[k] < 0.0) { hym &= ~(1u << k); ++cnt; }
+              if (v2 - iz[k] < 0.0) { hzm &= ~(1u << k); ++cnt; }
+              if (tt && v2 - it[k] < 0.0) { htm &= ~(1u << k); ++cnt; }
             }
             cnt = __reduce_add_sync(FULL, cnt);
             if (lane == 0) s_cnt[warp] = cnt;
@@ -177,14 +188,14 @@ __global__ void __launch_bounds__(MAXT) wide_sweep_kernel(const WideParams p) {
             old = total;
 #pragma unroll
             for (int k = 0; k < APT; ++k) {
-              if (!on[k]) continue;
-              double v = psi[k] + 0.5 * (xin[k] * cx[k] * (1.0 + hx[k]) +
-                                         iy[k] * cy[k] * (1.0 + hy[k]) +
-                                         iz[k] * cz[k] * (1.0 + hz[k]) +
-                                         it[k] * vd * (1.0 + ht[k]));
-              const double den = (v <= 0.0) ? 0.0
-                                            : sig + cx[k] * hx[k] + cy[k] * hy[k] +
-                                                  cz[k] * hz[k] + vd * ht[k];
+              const int a = angle(k);
+              if (a >= A) continue;
+              const double cx = s_cx[a], cy = s_cy[a], cz = s_cz[a];
+              const double hx = (hxm >> k) & 1u ? 1.0 : 0.0, hy = (hym >> k) & 1u ? 1.0 : 0.0,
+                           hz = (hzm >> k) & 1u ? 1.0 : 0.0, ht = (htm >> k) & 1u ? 1.0 : 0.0;
+              double v = source(k) + 0.5 * (xin[k] * cx * (1.0 + hx) + iy[k] * cy * (1.0 + hy) +
+                                           iz[k] * cz * (1.0 + hz) + it[k] * vd * (1.0 + ht));
+              const double den = (v <= 0.0) ? 0.0 : sig + cx * hx + cy * hy + cz * hz + vd * ht;
               pc[k] = den < 1.0e-12 ? 0.0 : __ddiv_rn(v, den);
             }
           }
@@ -193,15 +204,17 @@ __global__ void __launch_bounds__(MAXT) wide_sweep_kernel(const WideParams p) {
         double part0 = 0.0;
 #pragma unroll
         for (int k = 0; k < APT; ++k) {
-          if (!on[k]) continue;
-          const int a = ang[k];
+          const int a = angle(k);
+          if (a >= A) continue;
+          const double hx = (hxm >> k) & 1u ? 1.0 : 0.0, hy = (hym >> k) & 1u ? 1.0 : 0.0,
+                       hz = (hzm >> k) & 1u ? 1.0 : 0.0, ht = (htm >> k) & 1u ? 1.0 : 0.0;
           const double v2 = 2.0 * pc[k];
-          xin[k] = (v2 - xin[k]) * hx[k];
-          const double oy = (v2 - iy[k]) * hy[k], oz = (v2 - iz[k]) * hz[k];
+          xin[k] = (v2 - xin[k]) * hx;
+          const double oy = (v2 - iy[k]) * hy, oz = (v2 - iz[k]) * hz;
           ypen[(size_t)xx * A + a] = oy;
           zpl[((size_t)yy * nx + xx) * A + a] = oz;
-          if (tt) p.tf_out[(field + c) * A + a] = (v2 - it[k]) * ht[k];
-          part0 += wt[k] * pc[k];
+          if (tt) p.tf_out[(field + c) * A + a] = (v2 - it[k]) * ht;
+          part0 += s_w[a] * pc[k];
           // one-cell-wide meshes: the next cell's face is this cell's output
           if (nx == 1 && nyy > 0 && more) n_iy[k] = oy;
           if (nx == 1 && ny == 1 && nzz > 0 && more) n_iz[k] = oz;
@@ -219,8 +232,10 @@ __global__ void __launch_bounds__(MAXT) wide_sweep_kernel(const WideParams p) {
         for (int m = 1; m < M; ++m) {
           double pm = 0.0;
 #pragma unroll
-          for (int k = 0; k < APT; ++k)
-            if (on[k]) pm += ec[(size_t)m * A + ang[k]] * (wt[k] * pc[k]);
+          for (int k = 0; k < APT; ++k) {
+            const int a = angle(k);
+            if (a < A) pm += ec[(size_t)m * A + a] * (s_w[a] * pc[k]);
+          }
           pm += __shfl_xor_sync(FULL, pm, 16);
           pm += __shfl_xor_sync(FULL, pm, 8);
           pm += __shfl_xor_sync(FULL, pm, 4);
@@ -269,7 +284,7 @@ int wide_threads(int A) {
 }
 
 size_t wide_smem_bytes(int A, int nx, int M) {
-  return sizeof(double) * (size_t)(wide_threads(A) / 32) * nx * M;
+  return sizeof(double) * ((size_t)(wide_threads(A) / 32) * nx * M + 4 * (size_t)A);
 }
 
 bool wide_supported(int A, int nx, int M) {
