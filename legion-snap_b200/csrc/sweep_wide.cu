@@ -306,7 +306,7 @@ cudaError_t launch_sweep_wide(const WideParams &p, int n_blocks, cudaStream_t st
   if (!wide_supported(p.A, p.nx, p.M)) return cudaErrorInvalidValue;
   const int threads = wide_threads(p.A);
   const size_t smem = wide_smem_bytes(p.A, p.nx, p.M);
-  // register budgets: 255 per thread up to 256 threads, 128 beyond
+  // CTA sizes with their own instances (128 registers per thread in each)
   switch (wide_apt(p.A)) {
     case 1: return launch_apt<1, MAX_THREADS>(p, n_blocks, threads, smem, st);
     case 2:
