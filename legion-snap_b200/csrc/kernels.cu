@@ -16,6 +16,33 @@ inline int grid_for(long long n, int per_block = BLK) {
   return (int)(g < 1 ? 1 : g);
 }
 
+// Adds the CTA's count of violations and its largest change into the device
+// words with one atomic each instead of one per warp (every CTA thread calls
+// it; the launch is uniform in whether it does).  Non-negative floats order
+// like their bit patterns.
+__device__ __forceinline__ void flush_test(int bad, float dmax, int *violations, unsigned *maxdf) {
+  __shared__ int s_bad[32];
+  __shared__ unsigned s_max[32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  bad = __reduce_add_sync(0xffffffffu, bad);
+  const unsigned m = __reduce_max_sync(0xffffffffu, __float_as_uint(dmax));
+  if (lane == 0) {
+    s_bad[w] = bad;
+    s_max[w] = m;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int b = 0;
+    unsigned mm = 0;
+    for (int i = 0; i < nw; ++i) {
+      b += s_bad[i];
+      mm = s_max[i] > mm ? s_max[i] : mm;
+    }
+    if (b) atomicAdd(violations, b);
+    if (maxdf && mm) atomicMax(maxdf, mm);
+  }
+}
+
 __device__ __forceinline__ int band_of(int k) {
   int l = 0;
   while ((l + 1) * (l + 1) <= k) ++l;
@@ -278,10 +305,7 @@ __global__ void test_change_kernel(const double *__restrict__ flux, const double
     if (df > epsi) ++bad;
     dmax = fmaxf(dmax, (float)df);
   }
-  bad = __reduce_add_sync(0xffffffffu, bad);
-  if ((threadIdx.x & 31) == 0 && bad) atomicAdd(violations, bad);
-  const unsigned m = __reduce_max_sync(0xffffffffu, __float_as_uint(dmax));
-  if ((threadIdx.x & 31) == 0 && m) atomicMax(maxdf, m);
+  flush_test(bad, dmax, violations, maxdf);
 }
 
 // flux = sum of the octant slots.  With `test`, also the inner convergence
@@ -312,14 +336,7 @@ __global__ void reduce_slots_kernel(const ST *__restrict__ slots, int nslots, OT
     if (flux_out) flux_out[i] = (OT)s;
     if (flux64_out && (void *)flux64_out != (void *)flux_out) flux64_out[i] = s;
   }
-  if (test) {
-    bad = __reduce_add_sync(0xffffffffu, bad);
-    if ((threadIdx.x & 31) == 0 && bad) atomicAdd(violations, bad);
-    if (maxdf) {   // non-negative floats order like their bit patterns
-      const unsigned m = __reduce_max_sync(0xffffffffu, __float_as_uint(dmax));
-      if ((threadIdx.x & 31) == 0 && m) atomicMax(maxdf, m);
-    }
-  }
+  if (test) flush_test(bad, dmax, violations, maxdf);
 }
 
 // inner.cc:283-324 / outer.cc:354-403
@@ -338,8 +355,7 @@ __global__ void count_violations_kernel(const double *__restrict__ flux,
     df = fabs(flux[i * M] / p - df);
     if (df > epsi) ++bad;
   }
-  bad = __reduce_add_sync(0xffffffffu, bad);
-  if ((threadIdx.x & 31) == 0 && bad) atomicAdd(violations, bad);
+  flush_test(bad, 0.0f, violations, nullptr);
 }
 
 __global__ void copy_moment0_kernel(const double *__restrict__ flux, double *__restrict__ out,
